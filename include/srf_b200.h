@@ -1,0 +1,168 @@
+/*
+ * srf_b200 — C ABI of the B200 listmode PET projector library.
+ *
+ * Drop-in replacement for the native layer of SRF's listmode projector pair: the
+ * host launchers of src/cpp/tf_custom_ops/tor.cu.cc and siddon.cu.cc (paths relative
+ * to the SRF project root), which the TF op wrappers tor.cc / siddon.cc call.
+ *
+ * Conventions (all entry points):
+ *   - LOR data is the reference's column layout: one pointer per field. Event i of a
+ *     column is at column[i * lor_stride]; lor_stride = 1 is the reference's [C,N]
+ *     layout (tor.cc:140-160), lor_stride = C is a row-major [N,C] array.
+ *   - All data pointers are DEVICE pointers. grid / center / size are HOST arrays of
+ *     three values (kernel order: fastest axis first), passed by value to the kernel:
+ *     the reference instead copies them device-to-host on every call (tor.cu.cc:361).
+ *   - Image layout is [grid[2]][grid[1]][grid[0]] (grid[0] fastest), as the reference.
+ *   - Work is enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) and
+ *     never synchronises the host, so calls can be captured in a CUDA graph.
+ *   - Return value: SRF_OK or an srf_status_t code; nothing is launched on error.
+ *     srf_status_string() names it; srf_last_cuda_error() gives the CUDA error of the
+ *     calling thread's last failing call.
+ *   - Outputs are overwritten (the reference op zeroes them first: tor.cc:132,222,310,
+ *     siddon.cc:106) unless `accumulate` is non-zero, in which case results are added
+ *     to what the output already holds.
+ */
+#ifndef SRF_B200_H
+#define SRF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SRF_OK = 0,
+    SRF_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, non-finite geometry */
+    SRF_ERR_CUDA = 2,             /* a CUDA call failed; see srf_last_cuda_error() */
+    SRF_ERR_UNSUPPORTED = 3       /* parameters outside what the kernels support */
+} srf_status_t;
+
+const char *srf_status_string(int status);
+int srf_last_cuda_error(void);
+int srf_version(void);
+
+/* ------------------------------------------------------------------ TOR (tube of response)
+ * Field columns for TOR: x1,y1,z1,x2,y2,z2 (LOR endpoints, dominant axis last, as
+ * produced by recon_process, src/python/srf/preprocess/function/on_tor_lors.py:251-262),
+ * xc,yc,zc (TOF centre), sigma2_factor. TOF is on when tof_sigma2 < 405758
+ * (tor.cu.cc:20,84). tor_sigma2 = kernel_width^2/36 and the patch edge is
+ * ceil((sqrt(2)*kernel_width + voxel_z)/voxel_x) voxels (tor.cu.cc:374-375).
+ */
+
+/* Replaces projection(), tor.cu.cc:348-392 (TF op "Projection", tor.cc:14-28).
+ * projection_value[i] = sum over crossed slices and patch voxels of weight * image. */
+int srf_tor_projection(const float *x1, const float *y1, const float *z1, const float *x2,
+                       const float *y2, const float *z2, const float *xc, const float *yc,
+                       const float *zc, const float *sigma2_factor, int geo_sigma2_flag,
+                       float *projection_value, const int *grid, const float *center,
+                       const float *size, float kernel_width, float tof_bin, float tof_sigma2,
+                       const float *image, int64_t num_events, int64_t lor_stride,
+                       void *stream);
+
+/* Replaces backprojection(), tor.cu.cc:394-433 (TF op "Backprojection", tor.cc:30-47).
+ * image += weight / projection_value[i] for LORs with projection_value[i] > 1e-7. */
+int srf_tor_backprojection(const float *x1, const float *y1, const float *z1, const float *x2,
+                           const float *y2, const float *z2, const float *xc, const float *yc,
+                           const float *zc, const float *sigma2_factor, int geo_sigma2_flag,
+                           const float *projection_value, const int *grid, const float *center,
+                           const float *size, float kernel_width, float tof_bin,
+                           float tof_sigma2, float *image, int64_t num_events,
+                           int64_t lor_stride, int accumulate, void *stream);
+
+/* Replaces maplors(), tor.cu.cc:435-481 (TF op "Maplors", tor.cc:49-64): geometric
+ * weight only (no TOF), image += weight / projection_value[i] with no threshold. */
+int srf_tor_maplors(const float *x1, const float *y1, const float *z1, const float *x2,
+                    const float *y2, const float *z2, const float *sigma2_factor,
+                    int geo_sigma2_flag, const float *projection_value, const int *grid,
+                    const float *center, const float *size, float kernel_width, float *image,
+                    int64_t num_events, int64_t lor_stride, int accumulate, void *stream);
+
+/* No counterpart in the reference: the plain adjoint of srf_tor_projection,
+ * image += weight * values[i] (no division, no threshold). Backward pass of the
+ * differentiable projector and the OSEM numerator A^T(y/Ax) in its true form. */
+int srf_tor_backproject_adjoint(const float *x1, const float *y1, const float *z1,
+                                const float *x2, const float *y2, const float *z2,
+                                const float *xc, const float *yc, const float *zc,
+                                const float *sigma2_factor, int geo_sigma2_flag,
+                                const float *values, const int *grid, const float *center,
+                                const float *size, float kernel_width, float tof_bin,
+                                float tof_sigma2, float *image, int64_t num_events,
+                                int64_t lor_stride, int accumulate, void *stream);
+
+/* ---------------------------------------------------------------------------------- Siddon
+ * Field columns for Siddon: x1,y1,z1,x2,y2,z2,tof (tof in mm along the LOR, the
+ * reference's convention, siddon.cu.cc:460). Weight 1/L^2 (siddon.cu.cc:459). TOF on
+ * when tof_sigma2 < 405758 (siddon.cu.cc:15,308). A ray whose first voxel falls off
+ * the grid (the reference then reads outside the image) contributes nothing.
+ */
+
+/* Replaces projection(), siddon.cu.cc:583-606 (TF op "Projection", siddon.cc:14-26). */
+int srf_siddon_projection(const float *x1, const float *y1, const float *z1, const float *x2,
+                          const float *y2, const float *z2, const float *tof_t,
+                          float *projection_value, const int *grid, const float *center,
+                          const float *size, float tof_bin, float tof_sigma2,
+                          const float *image, int64_t num_events, int64_t lor_stride,
+                          void *stream);
+
+/* Replaces backprojection(), siddon.cu.cc:614-641 (TF op "Backprojection",
+ * siddon.cc:28-43): image += weight / projection_value[i] where projection_value[i] > 0. */
+int srf_siddon_backprojection(const float *x1, const float *y1, const float *z1,
+                              const float *x2, const float *y2, const float *z2,
+                              const float *tof_t, const float *projection_value,
+                              const int *grid, const float *center, const float *size,
+                              float tof_bin, float tof_sigma2, float *image,
+                              int64_t num_events, int64_t lor_stride, int accumulate,
+                              void *stream);
+
+/* Replaces maplors(), siddon.cu.cc:650-675 (TF op "Maplors", siddon.cc:45-57): weight
+ * 1/(L*L), no TOF, image += weight / projection_value[i] where projection_value[i] > 0. */
+int srf_siddon_maplors(const float *x1, const float *y1, const float *z1, const float *x2,
+                       const float *y2, const float *z2, const float *projection_value,
+                       const int *grid, const float *center, const float *size, float *image,
+                       int64_t num_events, int64_t lor_stride, int accumulate, void *stream);
+
+/* No counterpart in the reference: plain adjoint of srf_siddon_projection,
+ * image += weight * values[i]. */
+int srf_siddon_backproject_adjoint(const float *x1, const float *y1, const float *z1,
+                                   const float *x2, const float *y2, const float *z2,
+                                   const float *tof_t, const float *values, const int *grid,
+                                   const float *center, const float *size, float tof_bin,
+                                   float tof_sigma2, float *image, int64_t num_events,
+                                   int64_t lor_stride, int accumulate, void *stream);
+
+/* ------------------------------------------------------------------ LOR preprocessing
+ * The reference runs these in host numpy; here they run on the device with the same
+ * float32 arithmetic and the same output order (x group, y group, z group; in each,
+ * unswapped events then swapped ones, each in input order). Events with no dominant
+ * axis (NaN coordinates) are dropped. The caller provides `workspace` of at least
+ * srf_preprocess_workspace_size(num_events) bytes (device memory, 256-byte aligned).
+ * group_counts is a DEVICE int64[3] receiving the sizes of the x, y and z groups.
+ */
+int64_t srf_preprocess_workspace_size(int64_t num_events);
+
+/* Replaces recon_process, src/python/srf/preprocess/function/on_tor_lors.py:251-262:
+ * events [N, >=7] rows (x1,y1,z1,x2,y2,z2,tof) with row stride event_stride floats ->
+ * out [N, 10] rows (p1, p2, TOF centre, sigma2_factor; dominant axis last). tof_res is
+ * the TOF resolution in ps (cut to +/-3 sigma when < 10000). */
+int srf_recon_process(const float *events, int64_t num_events, int64_t event_stride,
+                      double tof_res, float *out, int64_t *group_counts, void *workspace,
+                      int64_t workspace_bytes, void *stream);
+
+/* Replaces map_process, on_tor_lors.py:243-248: lors [N, >=6] -> out [N, 7] rows
+ * (p1, p2 with the dominant axis last, sigma2_factor). */
+int srf_map_process(const float *lors, int64_t num_lors, int64_t lor_stride, float *out,
+                    int64_t *group_counts, void *workspace, int64_t workspace_bytes,
+                    void *stream);
+
+/* ------------------------------------------------------------------------- image algebra */
+
+/* MLEM/OSEM update of model/recon_step.py:48-49: image[v] *= effinv[v] * bp[v]. */
+int srf_mlem_update(float *image, const float *effinv, const float *bp, int64_t num_voxels,
+                    void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SRF_B200_H */

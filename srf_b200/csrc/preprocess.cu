@@ -1,0 +1,334 @@
+// LOR preprocessing on the GPU: the reference's host numpy pass
+// src/python/srf/preprocess/function/on_tor_lors.py (recon_process :251-262,
+// map_process :243-248) as three kernels.
+//
+// Per event (float32 arithmetic in numpy's operation order; numpy never fuses a*b+c,
+// so every product and sum here is a separately rounded __fmul_rn/__fadd_rn):
+//   f  = (dx^2+dy^2)^2 / (x1^2+x2^2+y1^2+y2^2) / L^2 / 2          (:137-166)
+//   dominant axis with the reference tie rules                      (:70-77)
+//   swap endpoints so the dominant coordinate grows, negating TOF    (:175-193)
+//   recon only: TOF centre C and the cut to C -/+ 3 sigma            (:196-229)
+//   column permutation that puts the dominant axis last              (:246-247, :259-260)
+//
+// Output order is the reference's: the x group, then y, then z; inside a group the
+// events that kept their orientation (ascending index), then the swapped ones
+// (ascending index) — np.intersect1d sorts, SwapPointsOrder vstacks positive/negative.
+// That is a stable partition into six buckets (axis, swapped), done with a per-tile
+// count, a scan over tiles and a stable scatter (ballot ranks inside each warp).
+
+#include "srf_common.cuh"
+
+namespace srf {
+namespace {
+
+constexpr int kThreads = 512;
+constexpr int kItems = 8;
+constexpr int kTile = kThreads * kItems;
+constexpr int kBuckets = 6;
+
+struct Rec {
+    float v[10];
+    int bucket;  // 0..5, or 6 when no axis is dominant (NaN input)
+};
+
+__device__ __forceinline__ float sq(float a) { return __fmul_rn(a, a); }
+
+__device__ __forceinline__ float pick(const float *a, int k) {
+    return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]);
+}
+
+// One event -> its bucket and output record. RECON selects recon_process (10
+// columns out) vs map_process (7 columns out).
+template <bool RECON>
+__device__ __forceinline__ Rec process(const float *e, bool cut, float limit) {
+    constexpr bool recon = RECON;
+    Rec r;
+    const float x1 = e[0], y1 = e[1], z1 = e[2], x2 = e[3], y2 = e[4], z2 = e[5];
+    const float t = recon ? e[6] : 0.0f;
+    const float dx = __fsub_rn(x2, x1), dy = __fsub_rn(y2, y1), dz = __fsub_rn(z2, z1);
+    // sigma2_factor
+    const float p_dis2 = __fadd_rn(__fadd_rn(sq(dx), sq(dy)), sq(dz));
+    const float dsq = __fadd_rn(sq(dx), sq(dy));
+    const float rsq = __fadd_rn(__fadd_rn(__fadd_rn(sq(x1), sq(x2)), sq(y1)), sq(y2));
+    const float f = __fdiv_rn(__fdiv_rn(__fdiv_rn(sq(dsq), rsq), p_dis2), 2.0f);
+    // dominant axis (dominentBy)
+    const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+    int axis;
+    if (ax >= ay && ax >= az) axis = 0;
+    else if (ay > ax && ay >= az) axis = 1;
+    else if (az > ax && az > ay) axis = 2;
+    else axis = -1;
+    if (axis < 0) {
+        r.bucket = kBuckets;
+        return r;
+    }
+    const float d = axis == 0 ? dx : (axis == 1 ? dy : dz);  // SwapPointsOrder's test
+    const bool swap = !(d >= 0.0f);
+    r.bucket = axis * 2 + (swap ? 1 : 0);
+    float p1[3] = {x1, y1, z1}, p2[3] = {x2, y2, z2};
+    float tt = t;
+    if (swap) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            float s = p1[k];
+            p1[k] = p2[k];
+            p2[k] = s;
+        }
+        tt = __fsub_rn(0.0f, t);
+    }
+    float c[3] = {0.f, 0.f, 0.f};
+    if (recon) {
+        // CutLoRs
+        float pd[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) pd[k] = __fsub_rn(p2[k], p1[k]);
+        const float p_dis = __fsqrt_rn(__fadd_rn(__fadd_rn(sq(pd[0]), sq(pd[1])), sq(pd[2])));
+        float dc[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) dc[k] = __fdiv_rn(pd[k], p_dis);
+        const float ratio = __fsub_rn(0.5f, __fdiv_rn(tt, p_dis));
+#pragma unroll
+        for (int k = 0; k < 3; k++) c[k] = __fadd_rn(__fmul_rn(ratio, pd[k]), p1[k]);
+        const float dcs = __fsqrt_rn(__fadd_rn(
+            __fadd_rn(sq(__fsub_rn(c[0], p1[0])), sq(__fsub_rn(c[1], p1[1]))),
+            sq(__fsub_rn(c[2], p1[2]))));
+        if (cut && dcs > limit) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const float m = __fmul_rn(limit, dc[k]);
+                p1[k] = __fsub_rn(c[k], m);
+                p2[k] = __fadd_rn(c[k], m);
+            }
+        }
+    }
+    // permutation: dominant axis last
+    const int a0 = axis == 0 ? 1 : 0;
+    const int a1 = axis == 2 ? 1 : 2;
+    const int a2 = axis;
+    r.v[0] = pick(p1, a0);
+    r.v[1] = pick(p1, a1);
+    r.v[2] = pick(p1, a2);
+    r.v[3] = pick(p2, a0);
+    r.v[4] = pick(p2, a1);
+    r.v[5] = pick(p2, a2);
+    if (recon) {
+        r.v[6] = pick(c, a0);
+        r.v[7] = pick(c, a1);
+        r.v[8] = pick(c, a2);
+        r.v[9] = f;
+    } else {
+        r.v[6] = f;
+    }
+    return r;
+}
+
+struct PreParams {
+    const float *events;
+    int64_t n, stride;
+    int recon, cut;
+    float limit;
+    unsigned char *bucket;   // [n]
+    int *tile_counts;        // [ntiles * kBuckets]
+    int64_t *tile_offsets;   // [ntiles * kBuckets]
+    int64_t *bucket_base;    // [kBuckets + 1]
+    int64_t *group_counts;   // [3] output
+    float *out;
+    int ntiles;
+};
+
+template <bool RECON>
+__global__ void __launch_bounds__(kThreads) classify_kernel(const PreParams p) {
+    __shared__ int counts[kBuckets];
+    if (threadIdx.x < kBuckets) counts[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kTile;
+    int local[kBuckets] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        const int64_t i = base + (int64_t)k * kThreads + threadIdx.x;
+        if (i < p.n) {
+            const Rec r = process<RECON>(p.events + i * p.stride, p.cut, p.limit);
+            p.bucket[i] = (unsigned char)r.bucket;
+#pragma unroll
+            for (int b = 0; b < kBuckets; b++) local[b] += (r.bucket == b);
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < kBuckets; b++) {
+        int v = local[b];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&counts[b], v);
+    }
+    __syncthreads();
+    if (threadIdx.x < kBuckets) p.tile_counts[blockIdx.x * kBuckets + threadIdx.x] = counts[threadIdx.x];
+}
+
+// One block: exclusive scan of the tile counts of each bucket, then of the bucket
+// totals; bucket_base[b] is where bucket b starts in the output.
+__global__ void __launch_bounds__(1024) scan_kernel(const PreParams p) {
+    __shared__ int64_t totals[kBuckets];
+    __shared__ int64_t warp_sums[32];
+    for (int b = 0; b < kBuckets; b++) {
+        int64_t carry = 0;
+        for (int start = 0; start < p.ntiles; start += blockDim.x) {
+            const int i = start + threadIdx.x;
+            int64_t v = i < p.ntiles ? p.tile_counts[i * kBuckets + b] : 0;
+            // inclusive scan inside the warp
+            int64_t x = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if ((threadIdx.x & 31) >= o) x += y;
+            }
+            if ((threadIdx.x & 31) == 31) warp_sums[threadIdx.x >> 5] = x;
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                int64_t w = threadIdx.x < (blockDim.x >> 5) ? warp_sums[threadIdx.x] : 0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+                    if (threadIdx.x >= o) w += y;
+                }
+                warp_sums[threadIdx.x] = w;
+            }
+            __syncthreads();
+            const int wid = threadIdx.x >> 5;
+            const int64_t before = (wid ? warp_sums[wid - 1] : 0) + carry;
+            if (i < p.ntiles) p.tile_offsets[i * kBuckets + b] = before + x - v;
+            const int64_t chunk = warp_sums[(blockDim.x >> 5) - 1];
+            __syncthreads();
+            carry += chunk;
+        }
+        if (threadIdx.x == 0) totals[b] = carry;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        int64_t acc = 0;
+        for (int b = 0; b < kBuckets; b++) {
+            p.bucket_base[b] = acc;
+            acc += totals[b];
+        }
+        p.bucket_base[kBuckets] = acc;
+        for (int a = 0; a < 3; a++) p.group_counts[a] = totals[2 * a] + totals[2 * a + 1];
+    }
+}
+
+template <bool RECON>
+__global__ void __launch_bounds__(kThreads) scatter_kernel(const PreParams p) {
+    __shared__ int warp_counts[kThreads / 32][kBuckets];
+    __shared__ int64_t running[kBuckets];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x < kBuckets)
+        running[threadIdx.x] =
+            p.bucket_base[threadIdx.x] + p.tile_offsets[blockIdx.x * kBuckets + threadIdx.x];
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kTile;
+    constexpr int ncols = RECON ? 10 : 7;
+    for (int k = 0; k < kItems; k++) {
+        const int64_t i = base + (int64_t)k * kThreads + threadIdx.x;
+        const int b = i < p.n ? (int)p.bucket[i] : kBuckets;
+        // rank among equal buckets inside the warp, in index order
+        int my_rank = 0;
+#pragma unroll
+        for (int q = 0; q < kBuckets; q++) {
+            const unsigned m = __ballot_sync(0xffffffffu, b == q);
+            if (b == q) my_rank = __popc(m & ((1u << lane) - 1u));
+            if (lane == 0) warp_counts[wid][q] = __popc(m);
+        }
+        __syncthreads();
+        int64_t dest = -1;
+        if (b < kBuckets) {
+            int64_t before = running[b];
+            for (int w = 0; w < wid; w++) before += warp_counts[w][b];
+            dest = before + my_rank;
+        }
+        __syncthreads();
+        if (threadIdx.x < kBuckets) {
+            int64_t add = 0;
+            for (int w = 0; w < kThreads / 32; w++) add += warp_counts[w][threadIdx.x];
+            running[threadIdx.x] += add;
+        }
+        if (dest >= 0) {
+            const Rec r = process<RECON>(p.events + i * p.stride, p.cut, p.limit);
+            float *o = p.out + dest * ncols;
+#pragma unroll
+            for (int c = 0; c < ncols; c++) o[c] = r.v[c];
+        }
+        __syncthreads();
+    }
+}
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+}  // namespace
+}  // namespace srf
+
+using namespace srf;
+
+extern "C" int64_t srf_preprocess_workspace_size(int64_t num_events) {
+    if (num_events < 0) return -1;
+    const int64_t ntiles = (num_events + kTile - 1) / kTile;
+    return (int64_t)(align256((size_t)num_events) + align256(sizeof(int) * ntiles * kBuckets) +
+                     align256(sizeof(int64_t) * ntiles * kBuckets) +
+                     align256(sizeof(int64_t) * (kBuckets + 1)));
+}
+
+namespace {
+int preprocess(const float *events, int64_t n, int64_t stride, int recon, double tof_res,
+               float *out, int64_t *group_counts, void *workspace, int64_t workspace_bytes,
+               cudaStream_t stream) {
+    if (n < 0 || !group_counts) return SRF_ERR_INVALID_ARGUMENT;
+    if (stride < (recon ? 7 : 6)) return SRF_ERR_INVALID_ARGUMENT;
+    if (n > 0 && (!events || !out || !workspace)) return SRF_ERR_INVALID_ARGUMENT;
+    if (workspace_bytes < srf_preprocess_workspace_size(n)) return SRF_ERR_INVALID_ARGUMENT;
+    if (!(tof_res == tof_res)) return SRF_ERR_INVALID_ARGUMENT;
+    PreParams p{};
+    p.events = events;
+    p.n = n;
+    p.stride = stride;
+    p.recon = recon;
+    p.cut = recon && tof_res < 10000.0;
+    p.limit = (float)(tof_res * 0.15 / 2.35482005 * 3);
+    p.ntiles = (int)((n + kTile - 1) / kTile);
+    char *w = static_cast<char *>(workspace);
+    p.bucket = reinterpret_cast<unsigned char *>(w);
+    w += align256((size_t)n);
+    p.tile_counts = reinterpret_cast<int *>(w);
+    w += align256(sizeof(int) * p.ntiles * kBuckets);
+    p.tile_offsets = reinterpret_cast<int64_t *>(w);
+    w += align256(sizeof(int64_t) * p.ntiles * kBuckets);
+    p.bucket_base = reinterpret_cast<int64_t *>(w);
+    p.group_counts = group_counts;
+    p.out = out;
+    if (n == 0) {
+        cudaError_t e = cudaMemsetAsync(group_counts, 0, 3 * sizeof(int64_t), stream);
+        if (e != cudaSuccess) {
+            set_cuda_error(e);
+            return SRF_ERR_CUDA;
+        }
+        return SRF_OK;
+    }
+    if (recon) {
+        classify_kernel<true><<<p.ntiles, kThreads, 0, stream>>>(p);
+        scan_kernel<<<1, 1024, 0, stream>>>(p);
+        scatter_kernel<true><<<p.ntiles, kThreads, 0, stream>>>(p);
+    } else {
+        classify_kernel<false><<<p.ntiles, kThreads, 0, stream>>>(p);
+        scan_kernel<<<1, 1024, 0, stream>>>(p);
+        scatter_kernel<false><<<p.ntiles, kThreads, 0, stream>>>(p);
+    }
+    return check_launch();
+}
+}  // namespace
+
+extern "C" int srf_recon_process(const float *events, int64_t num_events, int64_t event_stride,
+                                 double tof_res, float *out, int64_t *group_counts,
+                                 void *workspace, int64_t workspace_bytes, void *stream) {
+    return preprocess(events, num_events, event_stride, 1, tof_res, out, group_counts, workspace,
+                      workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" int srf_map_process(const float *lors, int64_t num_lors, int64_t lor_stride,
+                               float *out, int64_t *group_counts, void *workspace,
+                               int64_t workspace_bytes, void *stream) {
+    return preprocess(lors, num_lors, lor_stride, 0, 1.0e4, out, group_counts, workspace,
+                      workspace_bytes, (cudaStream_t)stream);
+}

@@ -1,0 +1,264 @@
+"""Tensor-level projector ops with the reference TF ops' argument lists.
+
+Each function mirrors one TF op of the reference and calls the matching C entry point:
+
+==========================  ======================================================
+``tor_projection``          TOR ``Projection``      (src/cpp/tf_custom_ops/tor.cc:14-28)
+``tor_backprojection``      TOR ``Backprojection``  (tor.cc:30-47)
+``tor_maplors``             TOR ``Maplors``         (tor.cc:49-64)
+``siddon_projection``       Siddon ``Projection``   (siddon.cc:14-26)
+``siddon_backprojection``   Siddon ``Backprojection`` (siddon.cc:28-43)
+``siddon_maplors``          Siddon ``Maplors``      (siddon.cc:45-57)
+``*_backproject_adjoint``   no reference counterpart: the plain transpose A^T v
+==========================  ======================================================
+
+``lors`` is a CUDA float32 tensor in the reference's ``[C, N]`` layout (one row per
+field, as the reference passes ``transpose(lors)``) or in the row-major ``[N, C]``
+layout that ``recon_process`` produces; ``layout`` says which ("auto" picks ``[C,N]``
+when the first dimension equals C, like the reference). ``image`` is in the kernel's
+layout ``[grid[2], grid[1], grid[0]]``; ``grid``/``center``/``size`` are three numbers
+each in kernel order (the reference passes ``image.grid[::-1]``). As in the reference,
+``image`` given to a back-projection or map op only provides the output's shape.
+
+There is no CPU path: every op requires CUDA tensors and the compiled library.
+"""
+
+import torch
+
+from . import _lib
+
+TOR_COLS = 10
+TOR_MAP_COLS = 7
+SIDDON_COLS = 7
+
+
+def _stream(device):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _check_cuda(*tensors):
+    dev = None
+    for t in tensors:
+        if t is None:
+            continue
+        if not isinstance(t, torch.Tensor) or not t.is_cuda:
+            raise TypeError("srf_b200 ops need CUDA tensors (there is no CPU path)")
+        if t.dtype != torch.float32:
+            raise TypeError(f"expected float32, got {t.dtype}")
+        if dev is None:
+            dev = t.device
+        elif t.device != dev:
+            raise ValueError("all tensors must be on the same device")
+    return dev
+
+
+def _columns(lors, ncols, layout="auto", min_cols=None):
+    """Column pointers + event stride for a [C,N] or [N,C] LOR tensor."""
+    if lors.dim() != 2:
+        raise ValueError(f"lors must be 2-D, got shape {tuple(lors.shape)}")
+    need = ncols if min_cols is None else min_cols
+    if layout == "auto":
+        layout = "cn" if lors.shape[0] in range(need, ncols + 1) else "nc"
+    if layout == "cn":
+        if lors.shape[0] < need:
+            raise ValueError(f"lors [C,N] needs {need} rows, got {lors.shape[0]}")
+        t = lors if lors.stride(1) == 1 else lors.contiguous()
+        n = t.shape[1]
+        base = t.data_ptr()
+        cols = [base + 4 * k * t.stride(0) for k in range(t.shape[0])]
+        return t, cols, n, 1
+    if layout == "nc":
+        if lors.shape[1] < need:
+            raise ValueError(f"lors [N,C] needs {need} columns, got {lors.shape[1]}")
+        t = lors if lors.stride(1) == 1 else lors.contiguous()
+        n = t.shape[0]
+        base = t.data_ptr()
+        cols = [base + 4 * k for k in range(t.shape[1])]
+        return t, cols, n, t.stride(0)
+    raise ValueError(f"unknown layout {layout!r}")
+
+
+def _geom(grid, center, size):
+    import ctypes as C
+    g = [int(v) for v in (grid.tolist() if torch.is_tensor(grid) else grid)]
+    c = [float(v) for v in (center.tolist() if torch.is_tensor(center) else center)]
+    s = [float(v) for v in (size.tolist() if torch.is_tensor(size) else size)]
+    if len(g) != 3 or len(c) != 3 or len(s) != 3:
+        raise ValueError("grid, center and size need three values each")
+    ga = (C.c_int * 3)(*g)
+    ca = (C.c_float * 3)(*c)
+    sa = (C.c_float * 3)(*s)
+    return g, ga, ca, sa
+
+
+def _image_shape(g):
+    return (g[2], g[1], g[0])
+
+
+def _as_image(image, g):
+    shape = _image_shape(g)
+    if image.numel() != shape[0] * shape[1] * shape[2]:
+        raise ValueError(f"image has {image.numel()} voxels, grid {g} needs "
+                         f"{shape[0] * shape[1] * shape[2]}")
+    return image.contiguous()
+
+
+def _values(v, n):
+    if v.numel() != n:
+        raise ValueError(f"lors_value has {v.numel()} entries for {n} LORs")
+    return v.reshape(-1).contiguous()
+
+
+def _out_image(out, g, like):
+    shape = _image_shape(g)
+    if out is None:
+        return torch.empty(shape, dtype=torch.float32, device=like.device), False
+    if tuple(out.shape) != shape and out.numel() != shape[0] * shape[1] * shape[2]:
+        raise ValueError("out has the wrong size")
+    if not out.is_contiguous():
+        raise ValueError("out must be contiguous")
+    return out, True
+
+
+# ----------------------------------------------------------------------------- TOR
+
+
+def tor_projection(lors, image, grid, center, size, kernel_width, geo_sigma2_flag=False,
+                   tof_bin=1.0e4, tof_sigma2=1.0e4, layout="auto", out=None):
+    dev = _check_cuda(lors, image, out)
+    t, cols, n, stride = _columns(lors, TOR_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    img = _as_image(image, g)
+    if out is None:
+        out = torch.empty(n, dtype=torch.float32, device=dev)
+    elif out.numel() != n or not out.is_contiguous():
+        raise ValueError("out must be a contiguous tensor with one entry per LOR")
+    with torch.cuda.device(dev):
+        _lib.call("srf_tor_projection", *cols[:10], int(bool(geo_sigma2_flag)), out.data_ptr(),
+                  ga, ca, sa, float(kernel_width), float(tof_bin), float(tof_sigma2),
+                  img.data_ptr(), n, stride, _stream(dev))
+    return out
+
+
+def _tor_scatter(fn, lors, values, image, grid, center, size, kernel_width, geo_sigma2_flag,
+                 tof_bin, tof_sigma2, layout, out, accumulate):
+    dev = _check_cuda(lors, values, image, out)
+    t, cols, n, stride = _columns(lors, TOR_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    v = _values(values, n)
+    res, _ = _out_image(out, g, lors)
+    with torch.cuda.device(dev):
+        _lib.call(fn, *cols[:10], int(bool(geo_sigma2_flag)), v.data_ptr(), ga, ca, sa,
+                  float(kernel_width), float(tof_bin), float(tof_sigma2), res.data_ptr(), n,
+                  stride, int(bool(accumulate) and out is not None), _stream(dev))
+    return res
+
+
+def tor_backprojection(image, lors, lors_value, grid, center, size, kernel_width,
+                       geo_sigma2_flag=False, tof_bin=1.0e4, tof_sigma2=1.0e4, layout="auto",
+                       out=None, accumulate=False):
+    """image + sum_i w_i / lors_value[i] over LORs with lors_value > 1e-7 (the
+    reference's ``Backprojection``; ``image`` only gives the shape)."""
+    return _tor_scatter("srf_tor_backprojection", lors, lors_value, image, grid, center, size,
+                        kernel_width, geo_sigma2_flag, tof_bin, tof_sigma2, layout, out,
+                        accumulate)
+
+
+def tor_backproject_adjoint(values, lors, grid, center, size, kernel_width,
+                            geo_sigma2_flag=False, tof_bin=1.0e4, tof_sigma2=1.0e4,
+                            layout="auto", out=None, accumulate=False):
+    """A^T values: the exact transpose of ``tor_projection``."""
+    return _tor_scatter("srf_tor_backproject_adjoint", lors, values, None, grid, center, size,
+                        kernel_width, geo_sigma2_flag, tof_bin, tof_sigma2, layout, out,
+                        accumulate)
+
+
+def tor_maplors(image, grid, center, size, lors, lors_value, kernel_width,
+                geo_sigma2_flag=False, layout="auto", out=None, accumulate=False):
+    """The reference's ``Maplors``: lors [7,N] (x1..z2, sigma2_factor), geometric
+    weight only, image += w / lors_value with no threshold."""
+    dev = _check_cuda(lors, lors_value, image, out)
+    t, cols, n, stride = _columns(lors, TOR_MAP_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    v = _values(lors_value, n)
+    res, _ = _out_image(out, g, lors)
+    with torch.cuda.device(dev):
+        _lib.call("srf_tor_maplors", *cols[:7], int(bool(geo_sigma2_flag)), v.data_ptr(), ga, ca,
+                  sa, float(kernel_width), res.data_ptr(), n, stride,
+                  int(bool(accumulate) and out is not None), _stream(dev))
+    return res
+
+
+# -------------------------------------------------------------------------- Siddon
+
+
+def siddon_projection(lors, image, grid, center, size, tof_bin=1.0e4, tof_sigma2=1.0e4,
+                      layout="auto", out=None):
+    dev = _check_cuda(lors, image, out)
+    t, cols, n, stride = _columns(lors, SIDDON_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    img = _as_image(image, g)
+    if out is None:
+        out = torch.empty(n, dtype=torch.float32, device=dev)
+    elif out.numel() != n or not out.is_contiguous():
+        raise ValueError("out must be a contiguous tensor with one entry per LOR")
+    with torch.cuda.device(dev):
+        _lib.call("srf_siddon_projection", *cols[:7], out.data_ptr(), ga, ca, sa,
+                  float(tof_bin), float(tof_sigma2), img.data_ptr(), n, stride, _stream(dev))
+    return out
+
+
+def _siddon_scatter(fn, lors, values, image, grid, center, size, tof_bin, tof_sigma2, layout,
+                    out, accumulate):
+    dev = _check_cuda(lors, values, image, out)
+    t, cols, n, stride = _columns(lors, SIDDON_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    v = _values(values, n)
+    res, _ = _out_image(out, g, lors)
+    with torch.cuda.device(dev):
+        _lib.call(fn, *cols[:7], v.data_ptr(), ga, ca, sa, float(tof_bin), float(tof_sigma2),
+                  res.data_ptr(), n, stride, int(bool(accumulate) and out is not None),
+                  _stream(dev))
+    return res
+
+
+def siddon_backprojection(image, lors, lors_value, grid, center, size, tof_bin=1.0e4,
+                          tof_sigma2=1.0e4, layout="auto", out=None, accumulate=False):
+    return _siddon_scatter("srf_siddon_backprojection", lors, lors_value, image, grid, center,
+                           size, tof_bin, tof_sigma2, layout, out, accumulate)
+
+
+def siddon_backproject_adjoint(values, lors, grid, center, size, tof_bin=1.0e4,
+                               tof_sigma2=1.0e4, layout="auto", out=None, accumulate=False):
+    return _siddon_scatter("srf_siddon_backproject_adjoint", lors, values, None, grid, center,
+                           size, tof_bin, tof_sigma2, layout, out, accumulate)
+
+
+def siddon_maplors(image, grid, center, size, lors, lors_value, layout="auto", out=None,
+                   accumulate=False):
+    """The reference's Siddon ``Maplors``: only x1..z2 of ``lors`` are read."""
+    dev = _check_cuda(lors, lors_value, image, out)
+    t, cols, n, stride = _columns(lors, SIDDON_COLS, layout, min_cols=6)
+    g, ga, ca, sa = _geom(grid, center, size)
+    v = _values(lors_value, n)
+    res, _ = _out_image(out, g, lors)
+    with torch.cuda.device(dev):
+        _lib.call("srf_siddon_maplors", *cols[:6], v.data_ptr(), ga, ca, sa, res.data_ptr(), n,
+                  stride, int(bool(accumulate) and out is not None), _stream(dev))
+    return res
+
+
+# --------------------------------------------------------------------- image algebra
+
+
+def mlem_update_(image, effinv, bp):
+    """In place: image *= effinv * bp (``mlem_update``, model/recon_step.py:48-49)."""
+    dev = _check_cuda(image, effinv, bp)
+    if not (image.is_contiguous() and effinv.is_contiguous() and bp.is_contiguous()):
+        raise ValueError("mlem_update_ needs contiguous tensors")
+    if not (image.numel() == effinv.numel() == bp.numel()):
+        raise ValueError("image, effinv and bp must have the same number of voxels")
+    with torch.cuda.device(dev):
+        _lib.call("srf_mlem_update", image.data_ptr(), effinv.data_ptr(), bp.data_ptr(),
+                  image.numel(), _stream(dev))
+    return image

@@ -1,0 +1,109 @@
+"""LOR preprocessing on the GPU: ``recon_process`` / ``map_process`` of
+``src/python/srf/preprocess/function/on_tor_lors.py:243-262`` and the effmap merge of
+``src/python/srf/preprocess/merge_map.py``.
+
+``recon_process(events, tof_res)`` and ``map_process(lors)`` return a dict
+``{'x': ..., 'y': ..., 'z': ...}`` of row-major CUDA tensors ([N_a, 10] / [N_a, 7]),
+views into one buffer, exactly the reference's dict of numpy arrays but resident on
+the device. The group sizes are read back to the host (one small copy).
+"""
+
+import numpy as np
+import torch
+
+from . import _lib
+from .data import ListModeData, ListModeDataSplit, ListModeDataSplitWithoutTOF, as_cuda_f32
+
+AXES = ("x", "y", "z")
+
+
+def _stream(dev):
+    return torch.cuda.current_stream(dev).cuda_stream
+
+
+def _run(fn, events, ncols_in, ncols_out, *extra):
+    ev = as_cuda_f32(events)
+    if ev.dim() != 2 or ev.shape[1] < ncols_in:
+        raise ValueError(f"expected [N, >={ncols_in}] events, got {tuple(ev.shape)}")
+    if ev.stride(1) != 1:
+        ev = ev.contiguous()
+    n = ev.shape[0]
+    dev = ev.device
+    lib = _lib.load()
+    ws_bytes = int(lib.srf_preprocess_workspace_size(n))
+    ws = torch.empty(max(ws_bytes, 256), dtype=torch.uint8, device=dev)
+    out = torch.empty((n, ncols_out), dtype=torch.float32, device=dev)
+    counts = torch.zeros(3, dtype=torch.int64, device=dev)
+    with torch.cuda.device(dev):
+        _lib.call(fn, ev.data_ptr(), n, ev.stride(0), *extra, out.data_ptr(), counts.data_ptr(),
+                  ws.data_ptr(), ws.numel(), _stream(dev))
+    c = counts.cpu().tolist()
+    groups, start = {}, 0
+    for a, k in zip(AXES, c):
+        groups[a] = out[start:start + k]
+        start += k
+    return groups
+
+
+def recon_process(events, tof_res):
+    """[N, 7] (x1,y1,z1,x2,y2,z2,tof) -> {'x','y','z'}: [N_a, 10]."""
+    return _run("srf_recon_process", events, 7, 10, float(tof_res))
+
+
+def map_process(lors):
+    """[N, 6] (x1..z2) -> {'x','y','z'}: [N_a, 7]."""
+    return _run("srf_map_process", lors, 6, 7)
+
+
+def split_listmode(groups, values=None, without_tof=False):
+    """Wrap recon/map_process output as the reference's loader does
+    (``SplitWorkerLoader.load``, src/python/srf/data/loader.py:96-119): values of one."""
+    parts = []
+    for a in AXES:
+        g = groups[a]
+        v = values[a] if values is not None else torch.ones(g.shape[0], dtype=torch.float32,
+                                                           device=g.device)
+        parts.append(ListModeData(g, v))
+    cls = ListModeDataSplitWithoutTOF if without_tof else ListModeDataSplit
+    return cls(*parts)
+
+
+# ------------------------------------------------------------------- effmap merge
+
+
+def crop_mask(grid, center, size, inner_radius, axial_length, crop_ratio=0.95):
+    """Keep-mask of ``crop_image`` (merge_map.py:47-65) over the [nx,ny,nz] image. The
+    reference pairs the mesh list of ``RingBlock.get_meshes`` (np.meshgrid 'xy' order:
+    iy, ix, iz) with the image flattened as (ix, iy, iz); the mask keeps that pairing."""
+    grid = np.asarray(grid)
+    center = np.asarray(center, dtype=np.float64)
+    size = np.asarray(size, dtype=np.float64)
+    interval = size / grid
+    p0 = center - (size - interval) / 2
+    p1 = center + (size - interval) / 2
+    r = [np.linspace(p0[i], p1[i], grid[i]) for i in range(3)]
+    m = np.array(np.meshgrid(r[0], r[1], r[2])).reshape((3, -1)).T
+    keep = np.ones(m.shape[0], bool)
+    keep[np.sqrt(m[:, 0] ** 2 + m[:, 1] ** 2) > crop_ratio * inner_radius] = False
+    keep[np.abs(m[:, 2]) >= axial_length / 2] = False
+    return keep.reshape(tuple(grid))
+
+
+def merge_effmap(total, keep, threshold=1e-6, zero_below=True):
+    """Crop, normalise to max 1 and invert a summed map (merge_map.py:37-41; with
+    ``threshold=1e-7, zero_below=False`` the ``merge_effmap_full`` variant :85-87).
+    ``total`` and ``keep`` are tensors on the same device; returns float32."""
+    m = torch.where(keep, total, torch.zeros_like(total)).to(torch.float64)
+    m = m / m.max()
+    hi = m > threshold
+    out = torch.where(hi, 1.0 / torch.where(hi, m, torch.ones_like(m)),
+                      torch.zeros_like(m) if zero_below else m)
+    return out.to(torch.float32)
+
+
+def initial_image(grid, center, size, inner_radius, axial_length, device, crop_ratio=0.95):
+    """``MasterLoader.create_image`` (src/python/srf/data/loader.py:28-37): ones,
+    cropped like the effmap."""
+    keep = torch.as_tensor(crop_mask(grid, center, size, inner_radius, axial_length,
+                                     crop_ratio), device=device)
+    return keep.to(torch.float32)
