@@ -1,0 +1,459 @@
+#!/usr/bin/env python
+"""Benchmark: TOF-TOR listmode projection + back-projection throughput (LORs/s).
+
+Workload (default): 128x128x64 image at 3.2 mm, ring scanner R = 400 mm with
+400 crystals x 32 rings (3.2 mm pitch), 10M seeded events from a cylinder phantom with
+four hot spheres, TOF 530 ps FWHM (tof_sigma2 = 1139.77 mm^2, 40 ps = 6 mm bins),
+TOR kernel_width 10.19 mm (FWHM 4 mm), geometry-sigma correction off. Events are
+synthetic (no public dataset is involved) and preprocessed on the GPU by
+``recon_process`` before the timed region.
+
+One step = the OSEM numerator pass the reference runs per iteration
+(model/recon_step.py:38-40): TOR projection of all three dominant-axis groups, then
+the reference's back-projection A^T(1/Ax) of all three groups into one image; with
+N > 1 GPUs each rank owns its own 10M events (weak scaling) and the back-projected
+images are summed with one NCCL all-reduce.
+
+* ``value``: LORs/s over all ranks with inputs resident in HBM (LOR records 400 MB per
+  rank, larger than the 126 MB L2, so no flush is needed between steps).
+* ``e2e``: the same metric through the public API from pinned HOST buffers: each step
+  copies the raw events host->device, preprocesses them, projects, back-projects and
+  copies the image back.
+* ``roofline``: the dominant kernel's algorithmic bytes per launch over its
+  CUDA-event duration inside the timed region (see DESIGN.md for the byte model).
+* ``cpu_baseline``: the reference's own projector sources compiled for the host
+  (oracle/_ref), all host threads, on a bounded sample of the same LORs.
+
+``--impl reference`` times that CPU reference as the reference arm.
+"""
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TOF-TOR proj+backproj LORs/s at 128x128x64 (10M events)"
+UNIT = "LORs/s"
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--events", type=int, default=None, help="override events per rank")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    return ap.parse_args(argv)
+
+
+# ------------------------------------------------------------------ distributed
+
+
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    """nvidia-smi sampling of the SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for _, _, flags in rows for k, f in enumerate(flags)
+                          if f.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# --------------------------------------------------------------------- workload
+
+
+def workload_inputs(events_per_rank, rank, device):
+    from srf_b200 import synthetic as S
+    from srf_b200.scanner import tof_info
+    wl = S.tor_128()
+    n = events_per_rank or wl.n_events
+    tof_bin, tof_sigma2 = tof_info(wl.tof_res_ps, wl.tof_bin_ps)
+    phantom = S.standard_phantom(half_length=wl.scanner.axial_length / 2)
+    events = S.generate_events(n, wl.scanner, phantom, seed=wl.seed + 7919 * rank,
+                               tof_sigma_mm=math.sqrt(tof_sigma2), device=device)
+    img = phantom.voxelize(wl.grid, wl.center, wl.size) + np.float32(0.05)
+    return wl, events, img, tof_bin, tof_sigma2
+
+
+def model_for(wl, tof_bin, tof_sigma2):
+    from srf_b200 import SplitLoRsModel
+    return SplitLoRsModel(wl.kernel_width, False, tof_sigma2=tof_sigma2, tof_bin=tof_bin)
+
+
+def algorithmic_work(model, data, image):
+    """Useful samples per group (voxels with non-zero weight), from the library's own
+    counting kernel, and LOR counts."""
+    from srf_b200 import ops
+    per = {}
+    for a in model.AXIS:
+        _, g, c, s = model.kernel_geometry(image, a)
+        cnt = ops.tor_count_samples(data[a].lors, g, c, s, model.kernel_width,
+                                    model.geo_sigma2_flag, layout="nc")
+        per[a] = {"lors": int(cnt.shape[1]), "useful": int(cnt[0].sum(dtype=torch.int64)),
+                  "slots": int(cnt[1].sum(dtype=torch.int64))}
+    return per
+
+
+# ------------------------------------------------------------------ CPU baseline
+
+
+def cpu_baseline(groups_host, wl, tof_bin, tof_sigma2, image_np, target_s):
+    """Time the reference's host-built projector pair on a bounded sample of the same
+    LORs with all host threads (oracle/_ref), falling back to the single-thread oracle
+    port. Returns the cpu_baseline object."""
+    from oracle import preprocess_ref as P
+    from oracle import pyoracle as O
+    ncpu = os.cpu_count() or 1
+    if O.ReferenceHost.available():
+        R = O.ReferenceHost()
+        kind, threads = "reference", ncpu
+
+        def pair(lors, img, g, c, s):
+            pv = R.tor_projection(lors, img, g, c, s, wl.kernel_width, False, tof_bin,
+                                  tof_sigma2, nthreads=threads)
+            R.tor_backprojection(lors, pv, g, c, s, wl.kernel_width, False, tof_bin,
+                                 tof_sigma2, nthreads=threads)
+    else:
+        kind, threads = "port", 1
+
+        def pair(lors, img, g, c, s):
+            pv = O.tor_projection(lors, img, g, c, s, wl.kernel_width, False, tof_bin,
+                                  tof_sigma2, mode="f32")
+            O.tor_backprojection(lors, pv, g, c, s, wl.kernel_width, False, tof_bin,
+                                 tof_sigma2, mode="f32")
+
+    views = {a: P.axis_view(image_np, wl.center, wl.size, a) for a in "xyz"}
+    total = sum(groups_host[a].shape[0] for a in "xyz")
+
+    def run(frac):
+        n_done, t0 = 0, time.perf_counter()
+        for a in "xyz":
+            k = max(1, int(groups_host[a].shape[0] * frac))
+            lors = np.ascontiguousarray(groups_host[a][:k].T)
+            img, g, c, s = views[a]
+            pair(lors, img, g, c, s)
+            n_done += k
+        return n_done, time.perf_counter() - t0
+
+    n0, t0 = run(2000.0 / total)  # calibration
+    frac = min(1.0, (2000.0 / total) * max(1.0, target_s / max(t0, 1e-3)))
+    n1, t1 = run(frac)
+    return {"value": n1 / t1, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{n1} LORs (first {frac * 100:.2f}% of each dominant-axis group of the "
+                      f"same preprocessed events), projection + back-projection, "
+                      f"{t1:.1f} s wall"}
+
+
+# ------------------------------------------------------------------ reference arm
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import preprocess_ref as P
+    from srf_b200 import synthetic as S
+    from srf_b200.scanner import tof_info
+    wl = S.tor_128()
+    tof_bin, tof_sigma2 = tof_info(wl.tof_res_ps, wl.tof_bin_ps)
+    phantom = S.standard_phantom(half_length=wl.scanner.axial_length / 2)
+    n_gen = 400_000
+    ev = S.generate_events(n_gen, wl.scanner, phantom, seed=wl.seed,
+                           tof_sigma_mm=math.sqrt(tof_sigma2)).numpy()
+    groups = P.recon_process(ev, wl.tof_res_ps)
+    img = phantom.voxelize(wl.grid, wl.center, wl.size) + np.float32(0.05)
+    base = cpu_baseline(groups, wl, tof_bin, tof_sigma2, img, target_s=2.0)
+    # each step: the same bounded sample size that calibration chose
+    n_per_step = int(base["sample"].split()[0])
+    frac = n_per_step / sum(groups[a].shape[0] for a in "xyz")
+    from oracle import pyoracle as O
+    views = {a: P.axis_view(img, wl.center, wl.size, a) for a in "xyz"}
+    use_ref = O.ReferenceHost.available()
+    R = O.ReferenceHost() if use_ref else None
+    threads = os.cpu_count() if use_ref else 1
+
+    def step():
+        n = 0
+        for a in "xyz":
+            k = max(1, int(groups[a].shape[0] * frac))
+            lors = np.ascontiguousarray(groups[a][:k].T)
+            im, g, c, s = views[a]
+            if use_ref:
+                pv = R.tor_projection(lors, im, g, c, s, wl.kernel_width, False, tof_bin,
+                                      tof_sigma2, nthreads=threads)
+                R.tor_backprojection(lors, pv, g, c, s, wl.kernel_width, False, tof_bin,
+                                     tof_sigma2, nthreads=threads)
+            else:
+                pv = O.tor_projection(lors, im, g, c, s, wl.kernel_width, False, tof_bin,
+                                      tof_sigma2)
+                O.tor_backprojection(lors, pv, g, c, s, wl.kernel_width, False, tof_bin,
+                                     tof_sigma2)
+            n += k
+        return n
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    n = sum(step() for _ in range(args.steps))
+    dt = time.perf_counter() - t0
+    value = n / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded events)", "impl": "reference",
+            "config": {"workload": wl.name, "grid": list(wl.grid), "voxel_mm": wl.voxel,
+                       "kernel_width": wl.kernel_width, "tof_res_ps": wl.tof_res_ps,
+                       "sample_lors_per_step": n // args.steps},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                             "kind": "reference" if use_ref else "port",
+                             "sample": f"{n // args.steps} LORs per step from the same "
+                                       f"preprocessed events"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------- ours
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    from srf_b200 import Image, backprojection, projection, profiling
+    from srf_b200 import preprocess as PP
+
+    wl, events, img_np, tof_bin, tof_sigma2 = workload_inputs(args.events, rank, dev)
+    n_events = events.shape[0]
+    model = model_for(wl, tof_bin, tof_sigma2)
+    groups = PP.recon_process(events, wl.tof_res_ps)
+    data = PP.split_listmode(groups)
+    image = Image(torch.as_tensor(img_np, device=dev), wl.center, wl.size)
+    n_lors = sum(data[a].lors.shape[0] for a in "xyz")
+    work = algorithmic_work(model, data, image)
+
+    def step():
+        p = projection(model, image, data)
+        bp = backprojection(model, p, image)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(bp.data)
+        return bp
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    timer = profiling.KernelTimer()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with timer:
+        start.record()
+        for _ in range(args.steps):
+            step()
+        end.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    clk = clocks.stop() if clocks else None
+    kern = timer.summary()
+    ms = max_over_ranks(ms, world)
+    total_lors = n_lors * world * args.steps
+    value = total_lors / (ms / 1e3)
+
+    # ---------------------------------------------------------------- e2e (public API)
+    e2e = None
+    if args.e2e_steps > 0:
+        host_events = events.cpu().pin_memory()
+        bi = host_events.numel() * 4
+        bo = int(np.prod(wl.grid)) * 4
+
+        def e2e_step():
+            ev = host_events.to(dev, non_blocking=True)
+            g = PP.recon_process(ev, wl.tof_res_ps)
+            d = PP.split_listmode(g)
+            p = projection(model, image, d)
+            bp = backprojection(model, p, image)
+            if world > 1:
+                import torch.distributed as dist
+                dist.all_reduce(bp.data)
+            return bp.data.cpu()
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        s1.record()
+        torch.cuda.synchronize()
+        e_ms = max_over_ranks(s0.elapsed_time(s1), world)
+        e2e = {"value": n_events * world * args.e2e_steps / (e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+               "ms_per_step": e_ms / args.e2e_steps,
+               "path": "pinned host events -> recon_process -> projection -> backprojection "
+                       "-> host image"}
+
+    # ---------------------------------------------------------------- roofline
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    useful = sum(w["useful"] for w in work.values())
+    rec = 40  # bytes of one preprocessed LOR record (10 float32)
+    alg = {"srf_tor_projection": n_lors * (rec + 4) + 4 * useful,
+           "srf_tor_backprojection": n_lors * (rec + 4) + 8 * useful}
+    roof = None
+    if kern:
+        dom = max(kern, key=lambda k: kern[k]["total_ms"])
+        launches = kern[dom]["launches"]
+        per_launch_bytes = alg.get(dom, 0) * args.steps / max(launches, 1)
+        achieved = per_launch_bytes / (kern[dom]["mean_ms"] / 1e3) / 1e9
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+        if os.path.exists(prof):
+            traffic = json.load(open(prof)).get(dom)
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
+                "peak_source": f"{peak_src} hbm_gbs (burst copy)",
+                "algorithmic_bytes_per_launch": per_launch_bytes,
+                "useful_samples_per_step": useful,
+                "kernel_ms": {k: {"launches": v["launches"], "mean_ms": v["mean_ms"],
+                                  "share": v["total_ms"] / sum(x["total_ms"] for x in kern.values())}
+                              for k, v in kern.items()}}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            gh = {a: groups[a].cpu().numpy() for a in "xyz"}
+            base = cpu_baseline(gh, wl, tof_bin, tof_sigma2, img_np, args.cpu_seconds)
+        except Exception as exc:  # reported, never fatal for the GPU number
+            base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
+                    "sample": f"unavailable: {exc}"}
+
+    gpu_launches = sum(v["launches"] for v in kern.values())
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded events from a cylinder phantom)",
+                "config": {"workload": wl.name, "grid": list(wl.grid), "voxel_mm": wl.voxel,
+                           "events_per_rank": int(n_events), "lors_per_rank": int(n_lors),
+                           "kernel_width": round(wl.kernel_width, 4), "tof_res_ps": wl.tof_res_ps,
+                           "tof_bin_mm": tof_bin, "tof_sigma2": tof_sigma2,
+                           "groups": {a: w["lors"] for a, w in work.items()},
+                           "parallelism": f"events sharded, {world} rank(s)",
+                           "l2": "inputs larger than L2 (400 MB LOR records per rank)"},
+                "roofline": roof, "cpu_baseline": base, "e2e": e2e,
+                "gpu_launches": gpu_launches, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

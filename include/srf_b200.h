@@ -90,6 +90,16 @@ int srf_tor_backproject_adjoint(const float *x1, const float *y1, const float *z
                                 float tof_sigma2, float *image, int64_t num_events,
                                 int64_t lor_stride, int accumulate, void *stream);
 
+/* No counterpart in the reference: per-LOR work counts of the TOR operator, used for
+ * the roofline (algorithmic samples) and for work estimation. counts[i] = patch voxels
+ * with non-zero weight (inside the 3-sigma tube), counts[num_events + i] = window
+ * voxels visited (the reference's loop-body count). counts: DEVICE int32[2*N]. */
+int srf_tor_count_samples(const float *x1, const float *y1, const float *z1, const float *x2,
+                          const float *y2, const float *z2, const float *sigma2_factor,
+                          int geo_sigma2_flag, const int *grid, const float *center,
+                          const float *size, float kernel_width, int *counts,
+                          int64_t num_events, int64_t lor_stride, void *stream);
+
 /* ---------------------------------------------------------------------------------- Siddon
  * Field columns for Siddon: x1,y1,z1,x2,y2,z2,tof (tof in mm along the LOR, the
  * reference's convention, siddon.cu.cc:460). Weight 1/L^2 (siddon.cu.cc:459). TOF on

@@ -333,3 +333,99 @@ class ReferenceHost:
         self.sid.ref_siddon_maplors(_ptr(lors), _ptr(v), n, _ptr(g), _ptr(c), _ptr(s),
                                     _ptr(out), nthreads)
         return out
+
+
+class ReferenceGPU:
+    """The reference's own CUDA kernels built for sm_100a (oracle/_ref/libref_*_gpu.so).
+
+    Takes torch CUDA tensors (data pointers are passed through). The reference
+    launchers synchronise the device; each call returns after its kernels finished.
+    Only run on inputs the oracle has checked (``siddon_counts`` reports rays whose
+    first voxel would fall off the grid, which the reference would read out of bounds)."""
+
+    def __init__(self):
+        tor = os.path.join(REF_DIR, "libref_tor_gpu.so")
+        sid = os.path.join(REF_DIR, "libref_siddon_gpu.so")
+        if not (os.path.exists(tor) and os.path.exists(sid)):
+            raise FileNotFoundError("reference GPU build missing (make -C oracle ref-gpu)")
+        self.tor = C.CDLL(tor)
+        self.sid = C.CDLL(sid)
+        geo = [_p, _p, _p]
+        self.tor.refgpu_tor_projection.argtypes = [_p, _i64] + geo + [_f, _int, _f, _f, _p, _p]
+        self.tor.refgpu_tor_backprojection.argtypes = [_p, _p, _i64] + geo + [_f, _int, _f, _f, _p]
+        self.tor.refgpu_tor_maplors.argtypes = [_p, _p, _i64] + geo + [_f, _int, _p]
+        self.sid.refgpu_siddon_projection.argtypes = [_p, _i64] + geo + [_f, _f, _p, _p]
+        self.sid.refgpu_siddon_backprojection.argtypes = [_p, _p, _i64] + geo + [_f, _f, _p]
+        self.sid.refgpu_siddon_maplors.argtypes = [_p, _p, _i64] + geo + [_p]
+
+    @staticmethod
+    def available():
+        return all(os.path.exists(os.path.join(REF_DIR, f))
+                   for f in ("libref_tor_gpu.so", "libref_siddon_gpu.so"))
+
+    @staticmethod
+    def _check(rc, what):
+        if rc != 0:
+            raise RuntimeError(f"reference GPU {what} failed with CUDA error {rc}")
+
+    def tor_projection(self, lors, image, grid, center, size, kw, geo, tof_bin, tof_sigma2):
+        import torch
+        n = lors.shape[1]
+        g, c, s = _geom(grid, center, size)
+        out = torch.empty(n, dtype=torch.float32, device=lors.device)
+        self._check(self.tor.refgpu_tor_projection(lors.data_ptr(), n, _ptr(g), _ptr(c), _ptr(s),
+                                                   kw, int(geo), tof_bin, tof_sigma2,
+                                                   image.data_ptr(), out.data_ptr()), "proj")
+        return out
+
+    def tor_backprojection(self, lors, values, grid, center, size, kw, geo, tof_bin,
+                           tof_sigma2):
+        import torch
+        n = lors.shape[1]
+        g, c, s = _geom(grid, center, size)
+        out = torch.empty(_image_shape(g), dtype=torch.float32, device=lors.device)
+        self._check(self.tor.refgpu_tor_backprojection(lors.data_ptr(), values.data_ptr(), n,
+                                                       _ptr(g), _ptr(c), _ptr(s), kw, int(geo),
+                                                       tof_bin, tof_sigma2, out.data_ptr()),
+                    "bproj")
+        return out
+
+    def tor_maplors(self, lors, values, grid, center, size, kw, geo):
+        import torch
+        n = lors.shape[1]
+        g, c, s = _geom(grid, center, size)
+        out = torch.empty(_image_shape(g), dtype=torch.float32, device=lors.device)
+        self._check(self.tor.refgpu_tor_maplors(lors.data_ptr(), values.data_ptr(), n, _ptr(g),
+                                                _ptr(c), _ptr(s), kw, int(geo), out.data_ptr()),
+                    "map")
+        return out
+
+    def siddon_projection(self, lors, image, grid, center, size, tof_bin, tof_sigma2):
+        import torch
+        n = lors.shape[1]
+        g, c, s = _geom(grid, center, size)
+        out = torch.empty(n, dtype=torch.float32, device=lors.device)
+        self._check(self.sid.refgpu_siddon_projection(lors.data_ptr(), n, _ptr(g), _ptr(c),
+                                                      _ptr(s), tof_bin, tof_sigma2,
+                                                      image.data_ptr(), out.data_ptr()), "proj")
+        return out
+
+    def siddon_backprojection(self, lors, values, grid, center, size, tof_bin, tof_sigma2):
+        import torch
+        n = lors.shape[1]
+        g, c, s = _geom(grid, center, size)
+        out = torch.empty(_image_shape(g), dtype=torch.float32, device=lors.device)
+        self._check(self.sid.refgpu_siddon_backprojection(lors.data_ptr(), values.data_ptr(), n,
+                                                          _ptr(g), _ptr(c), _ptr(s), tof_bin,
+                                                          tof_sigma2, out.data_ptr()), "bproj")
+        return out
+
+    def siddon_maplors(self, lors, values, grid, center, size):
+        import torch
+        n = lors.shape[1]
+        g, c, s = _geom(grid, center, size)
+        out = torch.empty(_image_shape(g), dtype=torch.float32, device=lors.device)
+        self._check(self.sid.refgpu_siddon_maplors(lors.data_ptr(), values.data_ptr(), n,
+                                                   _ptr(g), _ptr(c), _ptr(s), out.data_ptr()),
+                    "map")
+        return out

@@ -17,11 +17,14 @@
 //               roundings (the host compiler without FMA, i.e. the reference compiled
 //               for the CPU through oracle/shim). With contract = 0 the f32 mode is
 //               bit-identical to the reference compiled for the host; that pins it.
-//   * f64 mode  evaluates every weight and every sum in double. For TOR the discrete
-//               choices that the reference makes in float — which slices a LOR crosses
-//               (tor.cu.cc:30-33) and where the patch window starts (tor.cu.cc:135-136)
-//               — are taken from the f32 path, so the f64 result is the reference's
-//               operator evaluated exactly. For Siddon the whole ray walk runs in double.
+//   * f64 mode  the reference's operator evaluated exactly: every discrete choice the
+//               reference makes in float is taken from the f32 path (with nvcc's
+//               contraction) — for TOR which slices a LOR crosses (tor.cu.cc:30-33),
+//               where the patch window starts (:135-136) and the 3-sigma cut-off test
+//               (:71); for Siddon the voxel sequence of the walk (:302-330) and the
+//               TOF 3-sigma test (:314) — while every weight, length and sum is
+//               evaluated in double. The f64-vs-f32 difference is therefore pure
+//               floating-point error of the values, not a different discretisation.
 //
 // Loop orders follow the reference so that float sums round identically: TOR
 // projection per LOR over slices in ascending order (the host slice loop at
@@ -32,6 +35,7 @@
 // ([10,N] for TOR: x1,y1,z1,x2,y2,z2,xc,yc,zc,sigma2_factor; [7,N] for TOR map:
 // x1..z2,sigma2_factor; [7,N] for Siddon: x1..z2,tof).
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
@@ -178,15 +182,16 @@ inline float tor_map_smv_f32(float f, bool geo, float cross_x, float cross_y, fl
 }
 
 // Same weights in double.
+// `inside` is the reference's float cut-off decision for this voxel.
 inline double tor_smv_f64(double xc, double yc, double zc, double f, bool geo, double slice_z,
                           double tof_bin, double tof_sigma2, bool tof_on, double cross_x,
                           double cross_y, double mesh_x, double mesh_y, double ux, double uy,
-                          double tor_sigma2, bool with_tof) {
+                          double tor_sigma2, bool with_tof, bool inside) {
     double dx = cross_x - mesh_x, dy = cross_y - mesh_y;
     double r_cos = dx * ux + dy * uy;
     double d2 = dx * dx + dy * dy - r_cos * r_cos;
     double tsc = geo ? tor_sigma2 * f : tor_sigma2;
-    double value = d2 < 9.0 * tsc ? std::exp(-0.5 * d2 / tsc) : 0.0;
+    double value = inside ? std::exp(-0.5 * d2 / tsc) : 0.0;
     if (with_tof && tof_on) {
         double ax = xc - cross_x, ay = yc - cross_y, az = zc - slice_z;
         double d2_tof = ax * ax + ay * ay + az * az - d2;
@@ -245,6 +250,15 @@ inline float tor_mesh(float inter, int k, float bound) {
 // Mesh centre of MapLoopPatch (tor.cu.cc:235-236): float arithmetic.
 inline float tor_mesh_map(float inter, int k, float bound, bool c) {
     return madd(inter, (float)(0.5 + k), bound, c);
+}
+
+// The reference's cut-off decision (tor.cu.cc:57-71) in its device float arithmetic.
+inline bool tor_inside_f32(const TorGeom &g, const TorCross &x, int i0, int i1, float f,
+                           bool geo) {
+    float d2 = tor_d2_f32(x.cross_x, x.cross_y, tor_mesh(g.inter_x, i0, g.l_bound),
+                          tor_mesh(g.inter_y, i1, g.b_bound), x.dcos_x, x.dcos_y, true);
+    float tsc = geo ? g.tor_sigma2 * f : g.tor_sigma2;
+    return (double)d2 < 9.0 * (double)tsc;
 }
 
 // ---------------------------------------------------------------------------
@@ -380,11 +394,14 @@ inline void setup_component(const Box<T> &b, const Ray<T> &ray, int comp, RayCas
 // outside the grid while the walk would run (the reference then reads outside the
 // image; the new kernels skip such a ray, and the oracle reports it).
 template <typename T>
-inline bool setup_raycast(const Box<T> &b, Ray<T> &ray, RayCast<T> &rc, bool c) {
+inline bool setup_raycast(const Box<T> &b, Ray<T> &ray, RayCast<T> &rc, bool c,
+                          int *pos_out = nullptr) {
     for (int i = 0; i < 3; i++) ray.start[i] = ray.start[i] - (b.center[i] - b.size[i] / 2);
     int pos[3] = {0, 0, 0};
     for (int k = 0; k < 3; k++) setup_component<T>(b, ray, k, rc, pos[k], c);
     rc.boffs = pos[0] + b.grid[0] * (pos[1] + b.grid[1] * pos[2]);
+    if (pos_out)
+        for (int k = 0; k < 3; k++) pos_out[k] = pos[k];
     bool runs = rc.inBuf[0] * rc.inBuf[1] * rc.inBuf[2] != 0;
     bool inside = true;
     for (int k = 0; k < 3; k++) inside = inside && pos[k] >= 0 && pos[k] < b.grid[k];
@@ -452,6 +469,102 @@ inline void siddon_tof_terms_f32(float t_tof, float nextT, float last_t, float l
     s = std::sqrt(2.0 * M_PI * (double)sigma2);
 }
 
+
+// ---- f64 mode for Siddon: the float walk decides, a double shadow measures.
+
+// Entry/exit parameters of the ray in double, all three slabs (no early exit).
+inline void clip_all_f64(const Box<double> &b, Ray<double> &ray) {
+    double tmin = 0, tmax = ray.length;
+    for (int k = 0; k < 3; k++) {
+        double top = b.center[k] + b.size[k] / 2, bot = b.center[k] - b.size[k] / 2;
+        double p0 = ray.start[k], dp = ray.dir[k];
+        if (dp > 0) {
+            tmax = std::min(tmax, (top - p0) / dp);
+            tmin = std::max(tmin, (bot - p0) / dp);
+        } else if (dp < 0) {
+            tmax = std::min(tmax, (bot - p0) / dp);
+            tmin = std::max(tmin, (top - p0) / dp);
+        }
+    }
+    ray.min_t = tmin;
+    ray.max_t = tmax;
+}
+
+struct ShadowRay {
+    bool through = false, ok = true;
+    RayCast<float> rc;  // the reference's float walk state
+    double length = 0, min_t = 0, nextT[3] = {0, 0, 0}, deltaT[3] = {0, 0, 0};
+    float lengthf = 0, min_tf = 0;
+};
+
+inline ShadowRay shadow_setup(const Box<float> &bf, const Box<double> &bd, const SiddonLor &l) {
+    ShadowRay S;
+    Ray<float> rf = create_ray<float>(l.x1, l.y1, l.z1, l.x2, l.y2, l.z2, true);
+    S.lengthf = rf.length;
+    if (!through_image<float>(bf, rf)) return S;
+    S.through = true;
+    S.min_tf = rf.min_t;
+    int pos[3];
+    S.ok = setup_raycast<float>(bf, rf, S.rc, true, pos);
+    Ray<double> rd = create_ray<double>(l.x1, l.y1, l.z1, l.x2, l.y2, l.z2, true);
+    clip_all_f64(bd, rd);
+    S.length = rd.length;
+    S.min_t = rd.min_t;
+    for (int k = 0; k < 3; k++) {
+        double v_res = bd.size[k] / bd.grid[k];
+        double p0 = rd.start[k] - (bd.center[k] - bd.size[k] / 2);
+        double pt = rd.min_t * rd.dir[k] + p0;
+        double dir = rd.dir[k];
+        if (rf.dir[k] > 0.0f && dir != 0) {
+            S.nextT[k] = ((pos[k] + 1) * v_res - pt) / dir;
+            S.deltaT[k] = v_res / dir;
+        } else if (rf.dir[k] < 0.0f && dir != 0) {
+            S.nextT[k] = (pos[k] * v_res - pt) / dir;
+            S.deltaT[k] = -v_res / dir;
+        } else {
+            S.nextT[k] = std::numeric_limits<float>::max();
+            S.deltaT[k] = std::numeric_limits<float>::max();
+        }
+    }
+    return S;
+}
+
+// Walk the float state; cb(index, l_f, next_f, last_f, l_d, next_d, last_d).
+template <typename F>
+inline void shadow_walk(ShadowRay &S, F &&cb) {
+    RayCast<float> &rc = S.rc;
+    float last_t = 0;
+    double last_d = 0;
+    int stillin = rc.inBuf[0] * rc.inBuf[1] * rc.inBuf[2];
+    while (stillin) {
+        int i = argmin3<float>(rc.nextT);
+        cb(rc.boffs, rc.nextT[i] - last_t, rc.nextT[i], last_t, S.nextT[i] - last_d, S.nextT[i],
+           last_d);
+        last_t = rc.nextT[i];
+        last_d = S.nextT[i];
+        rc.nextT[i] += rc.deltaT[i];
+        S.nextT[i] += S.deltaT[i];
+        rc.boffs += rc.deltaBuf[i];
+        stillin = rc.inBuf[i] - 1;
+        rc.inBuf[i] = stillin;
+    }
+}
+
+// The TOF factor of one voxel: float 3-sigma decision (siddon.cu.cc:311-314 with
+// nvcc contraction), double value bin*exp(-t^2/2s^2)/sqrt(2 pi s^2).
+inline bool shadow_tof(float t_tof_f, double t_tof_d, float next_f, float last_f, float l_f,
+                       double next_d, double last_d, double l_d, float tof_sigma2,
+                       float tof_bin, double &factor) {
+    bool skip;
+    double e, sq;
+    siddon_tof_terms_f32(t_tof_f, next_f, last_f, l_f, tof_sigma2, tof_bin, true, skip, e, sq);
+    if (skip) return false;
+    double t = t_tof_d - 0.5 * (next_d + last_d);
+    double s2 = (double)tof_sigma2 + (l_d * l_d + (double)tof_bin * tof_bin) / 12.0;
+    factor = (double)tof_bin * std::exp(-0.5 * t * t / s2) / std::sqrt(2.0 * M_PI * s2);
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -510,7 +623,8 @@ void oracle_tor_projection_f64(const float *lors, int64_t n, const int *grid, co
                                        tof_on, xd.cross_x, xd.cross_y,
                                        g.d_inter_x * (i0 + 0.5) + g.d_l_bound,
                                        g.d_inter_y * (i1 + 0.5) + g.d_b_bound, xd.dcos_x,
-                                       xd.dcos_y, g.d_tor_sigma2, true);
+                                       xd.dcos_y, g.d_tor_sigma2, true,
+                                       tor_inside_f32(g, x, i0, i1, l.f, geo));
                 pv += v * (double)slice[idx];
             });
         }
@@ -571,7 +685,8 @@ void oracle_tor_backprojection_f64(const float *lors, const float *lors_value, i
                                        tof_on, xd.cross_x, xd.cross_y,
                                        g.d_inter_x * (i0 + 0.5) + g.d_l_bound,
                                        g.d_inter_y * (i1 + 0.5) + g.d_b_bound, xd.dcos_x,
-                                       xd.dcos_y, g.d_tor_sigma2, true);
+                                       xd.dcos_y, g.d_tor_sigma2, true,
+                                       tor_inside_f32(g, x, i0, i1, l.f, geo));
                 slice[idx] += v / pv;
             });
         }
@@ -627,7 +742,8 @@ void oracle_tor_maplors_f64(const float *lors, const float *lors_value, int64_t 
                 double v = tor_smv_f64(0, 0, 0, l.f, geo, szd, 0, 0, false, xd.cross_x,
                                        xd.cross_y, g.d_inter_x * (i0 + 0.5) + g.d_l_bound,
                                        g.d_inter_y * (i1 + 0.5) + g.d_b_bound, xd.dcos_x,
-                                       xd.dcos_y, g.d_tor_sigma2, false);
+                                       xd.dcos_y, g.d_tor_sigma2, false,
+                                       tor_inside_f32(g, x, i0, i1, l.f, geo));
                 slice[idx] += v / pv;
             });
         }
@@ -716,34 +832,32 @@ int64_t oracle_siddon_projection_f32(const float *lors, int64_t n, const int *gr
 int64_t oracle_siddon_projection_f64(const float *lors, int64_t n, const int *grid,
                                      const float *center, const float *size, float tof_bin,
                                      float tof_sigma2, const float *image, double *out) {
-    Box<double> box = make_box<double>(grid, center, size);
+    Box<float> bf = make_box<float>(grid, center, size);
+    Box<double> bd = make_box<double>(grid, center, size);
     bool tof_on = tof_sigma2 < kTofThreshold;
     int64_t bad = 0;
     for (int64_t t = 0; t < n; t++) {
         SiddonLor l = siddon_lor(lors, n, t);
-        Ray<double> ray = create_ray<double>(l.x1, l.y1, l.z1, l.x2, l.y2, l.z2, true);
-        if (!through_image<double>(box, ray)) {
-            out[t] = 0.0;
-            continue;
-        }
-        RayCast<double> rc;
-        if (!setup_raycast<double>(box, ray, rc, true)) {
+        ShadowRay S = shadow_setup(bf, bd, l);
+        out[t] = 0.0;
+        if (!S.through) continue;
+        if (!S.ok) {
             bad++;
-            out[t] = 0.0;
             continue;
         }
-        double weight = 1.0 / (ray.length * ray.length);
-        double t_tof = ray.length * 0.5 - ray.min_t - (double)l.tof;
+        double weight = 1.0 / (S.length * S.length);
+        float t_tof_f = (float)((double)S.lengthf * 0.5 - (double)S.min_tf - (double)l.tof);
+        double t_tof_d = S.length * 0.5 - S.min_t - (double)l.tof;
         double pv = 0.0;
-        walk<double>(rc, [&](int mi, double l_len, double next_t, double last_t) {
+        shadow_walk(S, [&](int mi, float lf, float nf, float la_f, double ld, double nd,
+                           double la_d) {
             if (tof_on) {
-                double tt = t_tof - 0.5 * (next_t + last_t);
-                double s2 = (double)tof_sigma2 + (l_len * l_len + (double)tof_bin * tof_bin) / 12.0;
-                if (tt * tt / s2 < 9.0)
-                    pv += image[mi] * weight * l_len * tof_bin * std::exp(-0.5 * tt * tt / s2) /
-                          std::sqrt(2.0 * M_PI * s2);
+                double fac;
+                if (shadow_tof(t_tof_f, t_tof_d, nf, la_f, lf, nd, la_d, ld, tof_sigma2, tof_bin,
+                               fac))
+                    pv += image[mi] * weight * ld * fac;
             } else {
-                pv += image[mi] * weight * l_len;
+                pv += image[mi] * weight * ld;
             }
         });
         out[t] = pv;
@@ -796,35 +910,34 @@ int64_t oracle_siddon_backprojection_f32(const float *lors, const float *lors_va
 int64_t oracle_siddon_backprojection_f64(const float *lors, const float *lors_value, int64_t n,
                                          const int *grid, const float *center, const float *size,
                                          float tof_bin, float tof_sigma2, double *image) {
-    Box<double> box = make_box<double>(grid, center, size);
+    Box<float> bf = make_box<float>(grid, center, size);
+    Box<double> bd = make_box<double>(grid, center, size);
     std::memset(image, 0, sizeof(double) * (int64_t)grid[0] * grid[1] * grid[2]);
     bool tof_on = tof_sigma2 < kTofThreshold;
     int64_t bad = 0;
     for (int64_t t = 0; t < n; t++) {
         SiddonLor l = siddon_lor(lors, n, t);
         double pv = lors_value[t];
-        if (!(pv > 0)) continue;
-        Ray<double> ray = create_ray<double>(l.x1, l.y1, l.z1, l.x2, l.y2, l.z2, true);
-        if (!through_image<double>(box, ray)) continue;
-        RayCast<double> rc;
-        if (!setup_raycast<double>(box, ray, rc, true)) {
+        if (!(lors_value[t] > 0)) continue;
+        ShadowRay S = shadow_setup(bf, bd, l);
+        if (!S.through) continue;
+        if (!S.ok) {
             bad++;
             continue;
         }
-        double weight = 1.0 / (ray.length * ray.length);
-        double t_tof = ray.length * 0.5 - ray.min_t - (double)l.tof;
-        walk<double>(rc, [&](int mi, double l_len, double next_t, double last_t) {
-            double value;
+        double weight = 1.0 / (S.length * S.length);
+        float t_tof_f = (float)((double)S.lengthf * 0.5 - (double)S.min_tf - (double)l.tof);
+        double t_tof_d = S.length * 0.5 - S.min_t - (double)l.tof;
+        shadow_walk(S, [&](int mi, float lf, float nf, float la_f, double ld, double nd,
+                           double la_d) {
             if (tof_on) {
-                double tt = t_tof - 0.5 * (next_t + last_t);
-                double s2 = (double)tof_sigma2 + (l_len * l_len + (double)tof_bin * tof_bin) / 12.0;
-                if (!(tt * tt / s2 < 9.0)) return;
-                value = weight * l_len * tof_bin * std::exp(-0.5 * tt * tt / s2) /
-                        std::sqrt(2.0 * M_PI * s2);
+                double fac;
+                if (shadow_tof(t_tof_f, t_tof_d, nf, la_f, lf, nd, la_d, ld, tof_sigma2, tof_bin,
+                               fac))
+                    image[mi] += weight * ld * fac / pv;
             } else {
-                value = weight * l_len;
+                image[mi] += weight * ld / pv;
             }
-            image[mi] += value / pv;
         });
     }
     return bad;
@@ -861,23 +974,23 @@ int64_t oracle_siddon_maplors_f32(const float *lors, const float *lors_value, in
 int64_t oracle_siddon_maplors_f64(const float *lors, const float *lors_value, int64_t n,
                                   const int *grid, const float *center, const float *size,
                                   double *image) {
-    Box<double> box = make_box<double>(grid, center, size);
+    Box<float> bf = make_box<float>(grid, center, size);
+    Box<double> bd = make_box<double>(grid, center, size);
     std::memset(image, 0, sizeof(double) * (int64_t)grid[0] * grid[1] * grid[2]);
     int64_t bad = 0;
     for (int64_t t = 0; t < n; t++) {
         SiddonLor l = siddon_lor(lors, n, t);
         double pv = lors_value[t];
-        if (!(pv > 0)) continue;
-        Ray<double> ray = create_ray<double>(l.x1, l.y1, l.z1, l.x2, l.y2, l.z2, true);
-        double weight = 1.0 / (ray.length * ray.length);
-        if (!through_image<double>(box, ray)) continue;
-        RayCast<double> rc;
-        if (!setup_raycast<double>(box, ray, rc, true)) {
+        if (!(lors_value[t] > 0)) continue;
+        ShadowRay S = shadow_setup(bf, bd, l);
+        if (!S.through) continue;
+        if (!S.ok) {
             bad++;
             continue;
         }
-        walk<double>(rc, [&](int mi, double l_len, double, double) {
-            image[mi] += weight * l_len / pv;
+        double weight = 1.0 / (S.length * S.length);
+        shadow_walk(S, [&](int mi, float, float, float, double ld, double, double) {
+            image[mi] += weight * ld / pv;
         });
     }
     return bad;

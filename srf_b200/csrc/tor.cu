@@ -27,7 +27,7 @@
 namespace srf {
 namespace {
 
-enum TorOp { kProj = 0, kBack = 1, kMap = 2, kAdj = 3 };
+enum TorOp { kProj = 0, kBack = 1, kMap = 2, kAdj = 3, kCount = 4 };
 
 struct TorParams {
     const float *x1, *y1, *z1, *x2, *y2, *z2, *xc, *yc, *zc, *f;
@@ -46,6 +46,7 @@ struct TorParams {
     const float *values;
     float *image_out;
     float *proj_out;
+    int *count_out;   // kCount: [n] voxels with non-zero weight, [n] window voxels visited
 };
 
 // slice_z of the reference launchers: float for projection (tor.cu.cc:380), a double
@@ -100,6 +101,7 @@ __global__ void __launch_bounds__(256) tor_kernel(const TorParams p) {
         // Candidate slices: every s whose plane lies strictly inside (z1, z2), with a
         // margin; each is then tested with the reference's own ratio.
         float acc = 0.0f;
+        int n_useful = 0, n_slots = 0;
         const float zlo = fminf(z1, z2), zhi = fmaxf(z1, z2);
         if (dz != 0.0f && zlo == zlo && zhi == zhi && fabsf(zhi - zlo) <= 3.0e38f) {
             const float flo = floorf((zlo - p.slice0_f) / p.inter_z) - 2.0f;
@@ -131,6 +133,7 @@ __global__ void __launch_bounds__(256) tor_kernel(const TorParams p) {
                 }
                 const int i_lo = max(0, -ix0), i_hi = min(p.patch, p.gx - ix0);
                 const int j_lo = max(0, -iy0), j_hi = min(p.patch, p.gy - iy0);
+                if (OP == kCount) n_slots += max(0, i_hi - i_lo) * max(0, j_hi - j_lo);
                 const int64_t base = (int64_t)s * slice_mesh;
                 for (int j = j_lo; j < j_hi; ++j) {
                     const int iy = iy0 + j;
@@ -147,7 +150,9 @@ __global__ void __launch_bounds__(256) tor_kernel(const TorParams p) {
                         const float d2 = __fmaf_rn(-rc, rc, __fmaf_rn(dx, dx, dy2));
                         if (d2 < cut) {
                             const float w = exp2f(fmaf(d2, k1, k0));
-                            if (OP == kProj) {
+                            if (OP == kCount) {
+                                n_useful++;
+                            } else if (OP == kProj) {
                                 acc = fmaf(w, __ldg(p.image_in + row + ix), acc);
                             } else {
                                 atomicAdd(p.image_out + row + ix, w * scale);
@@ -162,6 +167,17 @@ __global__ void __launch_bounds__(256) tor_kernel(const TorParams p) {
         if (OP == kProj) {
             acc = warp_sum(acc);
             if (lane == 0) p.proj_out[t] = acc * scale;
+        }
+        if (OP == kCount) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                n_useful += __shfl_xor_sync(0xffffffffu, n_useful, o);
+                n_slots += __shfl_xor_sync(0xffffffffu, n_slots, o);
+            }
+            if (lane == 0) {
+                p.count_out[t] = n_useful;
+                p.count_out[p.n + t] = n_slots;
+            }
         }
     }
 }
@@ -317,6 +333,25 @@ extern "C" int srf_tor_maplors(const float *x1, const float *y1, const float *z1
     p.values = projection_value;
     p.image_out = image;
     return tor_launch<kMap>(p, (cudaStream_t)stream);
+}
+
+extern "C" int srf_tor_count_samples(const float *x1, const float *y1, const float *z1,
+                                     const float *x2, const float *y2, const float *z2,
+                                     const float *sigma2_factor, int geo_sigma2_flag,
+                                     const int *grid, const float *center, const float *size,
+                                     float kernel_width, int *counts, int64_t num_events,
+                                     int64_t lor_stride, void *stream) {
+    TorParams p{};
+    int st = tor_setup(p, grid, center, size, kernel_width, 0.0f, 1.0e30f, num_events,
+                       lor_stride);
+    if (st != SRF_OK) return st;
+    if (num_events > 0 && !cols_ok({x1, y1, z1, x2, y2, z2, sigma2_factor, counts}))
+        return SRF_ERR_INVALID_ARGUMENT;
+    p.x1 = x1; p.y1 = y1; p.z1 = z1; p.x2 = x2; p.y2 = y2; p.z2 = z2;
+    p.f = sigma2_factor;
+    p.geo = geo_sigma2_flag != 0;
+    p.count_out = counts;
+    return tor_launch<kCount>(p, (cudaStream_t)stream);
 }
 
 extern "C" int srf_tor_backproject_adjoint(const float *x1, const float *y1, const float *z1,

@@ -25,7 +25,7 @@ There is no CPU path: every op requires CUDA tensors and the compiled library.
 
 import torch
 
-from . import _lib
+from . import _lib, profiling
 
 TOR_COLS = 10
 TOR_MAP_COLS = 7
@@ -34,6 +34,13 @@ SIDDON_COLS = 7
 
 def _stream(device):
     return torch.cuda.current_stream(device).cuda_stream
+
+
+def _call(dev, name, *args):
+    if profiling._ACTIVE:
+        with profiling.timed_call(name, torch.cuda.current_stream(dev)):
+            return _lib.call(name, *args)
+    return _lib.call(name, *args)
 
 
 def _check_cuda(*tensors):
@@ -134,7 +141,7 @@ def tor_projection(lors, image, grid, center, size, kernel_width, geo_sigma2_fla
     elif out.numel() != n or not out.is_contiguous():
         raise ValueError("out must be a contiguous tensor with one entry per LOR")
     with torch.cuda.device(dev):
-        _lib.call("srf_tor_projection", *cols[:10], int(bool(geo_sigma2_flag)), out.data_ptr(),
+        _call(dev, "srf_tor_projection", *cols[:10], int(bool(geo_sigma2_flag)), out.data_ptr(),
                   ga, ca, sa, float(kernel_width), float(tof_bin), float(tof_sigma2),
                   img.data_ptr(), n, stride, _stream(dev))
     return out
@@ -148,7 +155,7 @@ def _tor_scatter(fn, lors, values, image, grid, center, size, kernel_width, geo_
     v = _values(values, n)
     res, _ = _out_image(out, g, lors)
     with torch.cuda.device(dev):
-        _lib.call(fn, *cols[:10], int(bool(geo_sigma2_flag)), v.data_ptr(), ga, ca, sa,
+        _call(dev, fn, *cols[:10], int(bool(geo_sigma2_flag)), v.data_ptr(), ga, ca, sa,
                   float(kernel_width), float(tof_bin), float(tof_sigma2), res.data_ptr(), n,
                   stride, int(bool(accumulate) and out is not None), _stream(dev))
     return res
@@ -183,10 +190,25 @@ def tor_maplors(image, grid, center, size, lors, lors_value, kernel_width,
     v = _values(lors_value, n)
     res, _ = _out_image(out, g, lors)
     with torch.cuda.device(dev):
-        _lib.call("srf_tor_maplors", *cols[:7], int(bool(geo_sigma2_flag)), v.data_ptr(), ga, ca,
+        _call(dev, "srf_tor_maplors", *cols[:7], int(bool(geo_sigma2_flag)), v.data_ptr(), ga, ca,
                   sa, float(kernel_width), res.data_ptr(), n, stride,
                   int(bool(accumulate) and out is not None), _stream(dev))
     return res
+
+
+def tor_count_samples(lors, grid, center, size, kernel_width, geo_sigma2_flag=False,
+                      layout="auto"):
+    """Per-LOR (non-zero-weight voxels, window voxels visited) as int32 [2, N]: the
+    TOR operator's work, independent of the TOF setting."""
+    dev = _check_cuda(lors)
+    t, cols, n, stride = _columns(lors, TOR_COLS, layout, min_cols=TOR_MAP_COLS)
+    g, ga, ca, sa = _geom(grid, center, size)
+    counts = torch.empty((2, n), dtype=torch.int32, device=dev)
+    fcol = cols[9] if len(cols) >= 10 else cols[6]
+    with torch.cuda.device(dev):
+        _call(dev, "srf_tor_count_samples", *cols[:6], fcol, int(bool(geo_sigma2_flag)), ga, ca,
+                  sa, float(kernel_width), counts.data_ptr(), n, stride, _stream(dev))
+    return counts
 
 
 # -------------------------------------------------------------------------- Siddon
@@ -203,7 +225,7 @@ def siddon_projection(lors, image, grid, center, size, tof_bin=1.0e4, tof_sigma2
     elif out.numel() != n or not out.is_contiguous():
         raise ValueError("out must be a contiguous tensor with one entry per LOR")
     with torch.cuda.device(dev):
-        _lib.call("srf_siddon_projection", *cols[:7], out.data_ptr(), ga, ca, sa,
+        _call(dev, "srf_siddon_projection", *cols[:7], out.data_ptr(), ga, ca, sa,
                   float(tof_bin), float(tof_sigma2), img.data_ptr(), n, stride, _stream(dev))
     return out
 
@@ -216,7 +238,7 @@ def _siddon_scatter(fn, lors, values, image, grid, center, size, tof_bin, tof_si
     v = _values(values, n)
     res, _ = _out_image(out, g, lors)
     with torch.cuda.device(dev):
-        _lib.call(fn, *cols[:7], v.data_ptr(), ga, ca, sa, float(tof_bin), float(tof_sigma2),
+        _call(dev, fn, *cols[:7], v.data_ptr(), ga, ca, sa, float(tof_bin), float(tof_sigma2),
                   res.data_ptr(), n, stride, int(bool(accumulate) and out is not None),
                   _stream(dev))
     return res
@@ -243,7 +265,7 @@ def siddon_maplors(image, grid, center, size, lors, lors_value, layout="auto", o
     v = _values(lors_value, n)
     res, _ = _out_image(out, g, lors)
     with torch.cuda.device(dev):
-        _lib.call("srf_siddon_maplors", *cols[:6], v.data_ptr(), ga, ca, sa, res.data_ptr(), n,
+        _call(dev, "srf_siddon_maplors", *cols[:6], v.data_ptr(), ga, ca, sa, res.data_ptr(), n,
                   stride, int(bool(accumulate) and out is not None), _stream(dev))
     return res
 
@@ -259,6 +281,6 @@ def mlem_update_(image, effinv, bp):
     if not (image.numel() == effinv.numel() == bp.numel()):
         raise ValueError("image, effinv and bp must have the same number of voxels")
     with torch.cuda.device(dev):
-        _lib.call("srf_mlem_update", image.data_ptr(), effinv.data_ptr(), bp.data_ptr(),
+        _call(dev, "srf_mlem_update", image.data_ptr(), effinv.data_ptr(), bp.data_ptr(),
                   image.numel(), _stream(dev))
     return image

@@ -1,0 +1,207 @@
+"""MLEM / OSEM reconstruction and the efficiency-map pass on the GPU.
+
+Reference path (relative to the SRF project root):
+
+* ``ReconStep.kernel`` (src/python/srf/model/recon_step.py:33-41): projection, the
+  reference back-projection A^T(1/Ax), then ``mlem_update`` x <- x * effinv * bp
+  (:48-49). The list-mode measurement y = 1 is implicit in the division.
+* ``LocalReconstructionGraph.run`` (src/python/srf/graph/reconstruction/
+  local_reconstruction.py:44-51): one update per iteration over the whole list, the
+  image saved as ``{prefix}_{i}.npy`` after every iteration.
+* The efficiency map: ``Maplors`` over detector-pair LORs, summed over the three axis
+  groups (physics/split_lors.py:116-133), cropped, normalised and inverted
+  (preprocess/merge_map.py:8-88).
+
+Ordered subsets (the reference carries them only in unused graph classes,
+graph/reconstruction/master.py:122-162): subset k holds events k, k+S, k+2S, ... of
+every axis group, and its update uses S * effinv, i.e. the sensitivity split evenly
+over subsets. With S = 1 this is exactly the reference's full-list MLEM.
+
+One iteration (all subsets) can be captured in a CUDA graph: the library never
+synchronises the host, so the whole sequence of projector launches, image
+permutations and updates replays with one launch.
+"""
+
+import os
+
+import numpy as np
+import torch
+
+from . import ops
+from .data import Image, ListModeData, ListModeDataSplit
+from .physics import CompleteLoRsModel, SplitLoRsModel, backprojection, map_lors, projection
+from .preprocess import crop_mask, map_process, merge_effmap, split_listmode
+
+
+def mlem_update(image_prev, image_succ, efficiency_map):
+    """x * effinv * bp (recon_step.py:48-49) in place on a copy of ``image_prev``."""
+    out = image_prev.data.clone()
+    ops.mlem_update_(out, efficiency_map.data.contiguous(), image_succ.data.contiguous())
+    return Image(out, image_prev.center, image_prev.size)
+
+
+def mlem_update_normal(image_prev, image_succ, efficiency_map):
+    """x / effmap * bp (recon_step.py:52-53)."""
+    inv = torch.where(efficiency_map.data != 0, 1.0 / efficiency_map.data,
+                      torch.zeros_like(efficiency_map.data))
+    return mlem_update(image_prev, image_succ, Image(inv, efficiency_map.center,
+                                                     efficiency_map.size))
+
+
+class ReconStep:
+    """projection -> back-projection -> update (recon_step.py:17-45)."""
+
+    def __init__(self, model, update=mlem_update):
+        self.model = model
+        self.update = update
+
+    def __call__(self, image, efficiency_map, projection_data):
+        proj = projection(self.model, image, projection_data)
+        back = backprojection(self.model, proj, image)
+        return self.update(image, back, efficiency_map)
+
+
+# ------------------------------------------------------------------------- subsets
+
+
+def _take(t, k, s):
+    return t[k::s].contiguous() if s > 1 else t
+
+
+def make_subsets(data, n_subsets):
+    """Interleaved subsets of list-mode data (split or complete)."""
+    out = []
+    for k in range(n_subsets):
+        if isinstance(data, ListModeDataSplit):
+            out.append(ListModeDataSplit(*[
+                ListModeData(_take(data[a].lors, k, n_subsets),
+                             _take(data[a].values, k, n_subsets)) for a in "xyz"]))
+        else:
+            out.append(ListModeData(_take(data.lors, k, n_subsets),
+                                    _take(data.values, k, n_subsets)))
+    return out
+
+
+# ---------------------------------------------------------------------- efficiency map
+
+
+def efficiency_map(model, lors, grid, center, size, inner_radius, axial_length,
+                   chunk=16_000_000, crop_ratio=0.95, threshold=1e-6, zero_below=True):
+    """Inverted efficiency map from detector-pair LORs ([N, 6] CUDA tensor or a callable
+    returning chunks): Maplors summed over the axis groups (or Siddon map), cropped,
+    normalised to max 1 and inverted (merge_map.py:37-41)."""
+    dev = lors.device
+    total = torch.zeros(tuple(grid), dtype=torch.float32, device=dev)
+    img = Image(total, center, size)
+    n = lors.shape[0]
+    for s in range(0, n, chunk):
+        part = lors[s:s + chunk]
+        if isinstance(model, SplitLoRsModel):
+            groups = map_process(part)
+            data = split_listmode(groups, without_tof=True)
+        else:
+            from .data import ListModeDataWithoutTOF
+            data = ListModeDataWithoutTOF(part, torch.ones(part.shape[0], device=dev))
+        total.add_(map_lors(model, data, img).data)
+    keep = torch.as_tensor(crop_mask(grid, center, size, inner_radius, axial_length,
+                                     crop_ratio), device=dev)
+    return Image(merge_effmap(total, keep, threshold, zero_below), center, size), total
+
+
+# ---------------------------------------------------------------------- OSEM driver
+
+
+class OSEM:
+    """Ordered-subsets EM with optional CUDA-graph capture of each iteration.
+
+    ``data``: ListModeDataSplit (TOR) or ListModeData (Siddon) with values of one.
+    ``effinv``: inverted efficiency map (Image). ``x0``: initial image (Image)."""
+
+    def __init__(self, model, data, effinv, x0, n_subsets=1, use_graph=False):
+        self.model = model
+        self.n_subsets = int(n_subsets)
+        self.subsets = make_subsets(data, self.n_subsets)
+        self.effinv = Image((effinv.data * float(self.n_subsets)).contiguous(), effinv.center,
+                            effinv.size)
+        self.x = Image(x0.data.clone().contiguous(), x0.center, x0.size)
+        self.use_graph = use_graph
+        self._graph = None
+        self.iteration = 0
+
+    def _subset_update(self, k):
+        proj = projection(self.model, self.x, self.subsets[k])
+        back = backprojection(self.model, proj, self.x)
+        ops.mlem_update_(self.x.data, self.effinv.data, back.data)
+
+    def _iterate(self):
+        for k in range(self.n_subsets):
+            self._subset_update(k)
+
+    def _capture(self):
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        backup = self.x.data.clone()
+        with torch.cuda.stream(s):
+            self._iterate()  # warm-up outside the graph (allocator, lazy init)
+        torch.cuda.current_stream().wait_stream(s)
+        self.x.data.copy_(backup)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._iterate()
+        self.x.data.copy_(backup)
+        self._graph = g
+
+    def step(self):
+        """One full iteration over all subsets."""
+        if self.use_graph:
+            if self._graph is None:
+                self._capture()
+            self._graph.replay()
+        else:
+            self._iterate()
+        self.iteration += 1
+        return self.x
+
+    def run(self, n_iterations, prefix=None, callback=None):
+        for _ in range(n_iterations):
+            self.step()
+            if prefix is not None:
+                save_checkpoint(prefix, self.iteration - 1, self.x)
+            if callback is not None:
+                callback(self.iteration, self.x)
+        return self.x
+
+
+# ----------------------------------------------------------------- checkpoint/resume
+
+
+def save_checkpoint(prefix, iteration, image, seed=None):
+    """``{prefix}_{i}.npy`` as the reference writes (local_reconstruction.py:50-51),
+    plus ``{prefix}_{i}.meta.npz`` with the iteration, center, size and seed."""
+    arr = image.data.detach().cpu().numpy()
+    np.save(f"{prefix}_{iteration}.npy", arr)
+    np.savez(f"{prefix}_{iteration}.meta.npz", iteration=iteration,
+             center=np.array(image.center), size=np.array(image.size),
+             seed=np.array(-1 if seed is None else seed))
+
+
+def latest_checkpoint(prefix):
+    """(iteration, path) of the newest ``{prefix}_{i}.npy``, or (None, None)."""
+    d = os.path.dirname(prefix) or "."
+    base = os.path.basename(prefix) + "_"
+    best = None
+    for f in os.listdir(d):
+        if f.startswith(base) and f.endswith(".npy"):
+            mid = f[len(base):-4]
+            if mid.isdigit() and (best is None or int(mid) > best[0]):
+                best = (int(mid), os.path.join(d, f))
+    return best if best else (None, None)
+
+
+def resume(prefix, center, size, device):
+    """Image and next iteration index from the newest checkpoint (or (None, 0))."""
+    it, path = latest_checkpoint(prefix)
+    if it is None:
+        return None, 0
+    arr = np.load(path)
+    return Image(torch.as_tensor(arr, device=device), center, size), it + 1

@@ -1,0 +1,59 @@
+"""The C-ABI library builds, loads without a GPU and exports exactly what
+include/srf_b200.h declares (no compute calls: this runs on CPU-only machines)."""
+
+import ctypes
+import os
+import re
+
+from srf_b200 import _lib, build
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "srf_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(srf_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ("srf_tor_projection", "srf_tor_backprojection", "srf_tor_maplors",
+              "srf_siddon_projection", "srf_siddon_backprojection", "srf_siddon_maplors",
+              "srf_recon_process", "srf_map_process"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    assert os.path.exists(build.LIBPATH)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_binding_covers_header():
+    assert set(declared_symbols()) == set(_lib.exported_symbols())
+
+
+def test_status_strings_without_gpu():
+    lib = _lib.load()
+    assert lib.srf_status_string(0) == b"ok"
+    assert lib.srf_status_string(1) == b"invalid argument"
+    assert lib.srf_version() >= 1
+
+
+def test_invalid_arguments_rejected_before_any_launch():
+    """Argument validation happens on the host and returns a status; nothing is
+    launched, so this is safe without a GPU."""
+    lib = _lib.load()
+    g = (ctypes.c_int * 3)(0, 4, 4)  # grid[0] = 0 is invalid
+    c = (ctypes.c_float * 3)(0, 0, 0)
+    s = (ctypes.c_float * 3)(1, 1, 1)
+    st = lib.srf_tor_projection(*([None] * 10), 0, None, g, c, s, 1.0, 1.0, 1.0, None, 0, 1,
+                                None)
+    assert st == 1
+    g2 = (ctypes.c_int * 3)(4, 4, 4)
+    st = lib.srf_siddon_projection(*([None] * 7), None, g2, c, s, 1.0, 1.0, None, -1, 1, None)
+    assert st == 1
+    assert lib.srf_preprocess_workspace_size(-1) == -1
+    assert lib.srf_preprocess_workspace_size(10) > 0
