@@ -344,11 +344,13 @@ def main(argv=None):
         clocks.start()
     timer = profiling.KernelTimer()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("bench_timed")
     with timer:
         start.record()
         for _ in range(args.steps):
             step()
         end.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()

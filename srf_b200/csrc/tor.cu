@@ -20,7 +20,10 @@
 // is applied once per LOR. Voxels outside the 3-sigma cut-off are skipped: their
 // weight is exactly zero in the reference as well.
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstdlib>
 
 #include "srf_common.cuh"
 
@@ -47,6 +50,7 @@ struct TorParams {
     float *image_out;
     float *proj_out;
     int *count_out;   // kCount: [n] voxels with non-zero weight, [n] window voxels visited
+    int use_slab;     // scatter ops: shared-memory slab kernel (1) or global atomics (0)
 };
 
 // slice_z of the reference launchers: float for projection (tor.cu.cc:380), a double
@@ -58,127 +62,412 @@ __device__ __forceinline__ float slice_z(const TorParams &p, int s) {
     return __double2float_rn(p.slice0_d + (double)step);
 }
 
+// 2^x with the hardware approximation (ex2.approx, relative error ~2^-22); the
+// argument here is always <= ~0, results below 2^-126 flush to zero.
+__device__ __forceinline__ float fast_exp2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Generic per-LOR body (any patch size): the reference's loops as written, every
+// in-slice window voxel visited. Used for patch sizes without a specialised kernel and
+// for map calls whose divisor is zero or non-finite.
+template <int OP>
+__device__ __noinline__ void generic_lor(const TorParams &p, int64_t t, int lane) {
+    const int64_t slice_mesh = (int64_t)p.gx * p.gy;
+    const int64_t o = t * p.stride;
+    const float x1 = __ldg(p.x1 + o), y1 = __ldg(p.y1 + o), z1 = __ldg(p.z1 + o);
+    const float x2 = __ldg(p.x2 + o), y2 = __ldg(p.y2 + o), z2 = __ldg(p.z2 + o);
+    const float f = __ldg(p.f + o);
+
+    // Per-LOR output scale and the early-outs of the reference's value tests.
+    float scale = p.tof_scale;
+    bool all_slots = false;  // map with a zero/non-finite divisor: every visited voxel gets w/v
+    if (OP == kBack) {
+        float v = __ldg(p.values + t);
+        if (!((double)v > 1e-7)) return;  // tor.cu.cc:203
+        scale = __fdiv_rn(p.tof_scale, v);
+    } else if (OP == kMap) {
+        float v = __ldg(p.values + t);
+        scale = __fdiv_rn(1.0f, v);  // tor.cu.cc:239 divides without a threshold
+        all_slots = !(fabsf(scale) <= 3.0e38f);
+    } else if (OP == kAdj) {
+        scale = p.tof_scale * __ldg(p.values + t);
+    }
+
+    const float d0 = __fsub_rn(x2, x1), d1 = __fsub_rn(y2, y1), dz = __fsub_rn(z2, z1);
+    const float dis = __fsqrt_rn(__fmaf_rn(dz, dz, __fmaf_rn(d0, d0, __fmul_rn(d1, d1))));
+    const float ux = __fdiv_rn(d0, dis), uy = __fdiv_rn(d1, dis);
+
+    float cut = p.cut, k1 = p.k1;
+    if (p.geo) {
+        const float tsc = __fmul_rn(p.tor_sigma2, f);  // tor.cu.cc:67
+        cut = __double2float_ru(9.0 * (double)tsc);
+        const float inv = 0.5f * kLog2e / tsc;
+        k1 = (p.tof_on && OP != kMap) ? (p.a_coef - inv) : -inv;
+    }
+
+    // Candidate slices: every s whose plane lies strictly inside (z1, z2), with a
+    // margin; each is then tested with the reference's own ratio.
+    float acc = 0.0f;
+    int n_useful = 0, n_slots = 0;
+    const float zlo = fminf(z1, z2), zhi = fmaxf(z1, z2);
+    if (dz != 0.0f && zlo == zlo && zhi == zhi && fabsf(zhi - zlo) <= 3.0e38f) {
+        const float flo = floorf((zlo - p.slice0_f) / p.inter_z) - 2.0f;
+        const float fhi = ceilf((zhi - p.slice0_f) / p.inter_z) + 2.0f;
+        const int s_lo = (int)fmaxf(flo, 0.0f);
+        const int s_hi = (int)fminf(fhi, (float)(p.gz - 1));
+        float xc = 0.f, yc = 0.f, zc = 0.f;
+        if (OP != kMap && p.tof_on) {
+            xc = __ldg(p.xc + o);
+            yc = __ldg(p.yc + o);
+            zc = __ldg(p.zc + o);
+        }
+        for (int s = s_lo + lane; s <= s_hi; s += 32) {
+            const float sz = slice_z<OP>(p, s);
+            const float ratio = __fdiv_rn(__fsub_rn(sz, z1), dz);
+            if (!(ratio > 0.0f && ratio < 1.0f)) continue;
+            const float cx = __fmaf_rn(d0, ratio, x1);
+            const float cy = __fmaf_rn(d1, ratio, y1);
+            const int ix0 =
+                __float2int_rz(__fdiv_rn(__fsub_rn(cx, p.l_bound), p.inter_x)) - p.half;
+            const int iy0 =
+                __float2int_rz(__fdiv_rn(__fsub_rn(cy, p.b_bound), p.inter_y)) - p.half;
+            float k0 = 0.0f;
+            if (OP != kMap && p.tof_on) {
+                const float ax = __fsub_rn(xc, cx), ay = __fsub_rn(yc, cy),
+                            az = __fsub_rn(zc, sz);
+                const float a2 = __fmaf_rn(az, az, __fmaf_rn(ax, ax, __fmul_rn(ay, ay)));
+                k0 = -a2 * p.a_coef;
+            }
+            const int i_lo = max(0, -ix0), i_hi = min(p.patch, p.gx - ix0);
+            const int j_lo = max(0, -iy0), j_hi = min(p.patch, p.gy - iy0);
+            if (OP == kCount) n_slots += max(0, i_hi - i_lo) * max(0, j_hi - j_lo);
+            const int64_t base = (int64_t)s * slice_mesh;
+            for (int j = j_lo; j < j_hi; ++j) {
+                const int iy = iy0 + j;
+                const float my = __fmaf_rn(p.inter_y, (float)iy + 0.5f, p.b_bound);
+                const float dy = __fsub_rn(cy, my);
+                const float dyuy = __fmul_rn(dy, uy);
+                const float dy2 = __fmul_rn(dy, dy);
+                const int64_t row = base + (int64_t)iy * p.gx;
+                for (int i = i_lo; i < i_hi; ++i) {
+                    const int ix = ix0 + i;
+                    const float mx = __fmaf_rn(p.inter_x, (float)ix + 0.5f, p.l_bound);
+                    const float dx = __fsub_rn(cx, mx);
+                    const float rc = __fmaf_rn(dx, ux, dyuy);
+                    const float d2 = __fmaf_rn(-rc, rc, __fmaf_rn(dx, dx, dy2));
+                    if (d2 < cut) {
+                        const float w = exp2f(fmaf(d2, k1, k0));
+                        if (OP == kCount) {
+                            n_useful++;
+                        } else if (OP == kProj) {
+                            acc = fmaf(w, __ldg(p.image_in + row + ix), acc);
+                        } else {
+                            atomicAdd(p.image_out + row + ix, w * scale);
+                        }
+                    } else if (OP == kMap && all_slots) {
+                        atomicAdd(p.image_out + row + ix, 0.0f * scale);
+                    }
+                }
+            }
+        }
+    }
+    if (OP == kProj) {
+        acc = warp_sum(acc);
+        if (lane == 0) p.proj_out[t] = acc * scale;
+    }
+    if (OP == kCount) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            n_useful += __shfl_xor_sync(0xffffffffu, n_useful, o);
+            n_slots += __shfl_xor_sync(0xffffffffu, n_slots, o);
+        }
+        if (lane == 0) {
+            p.count_out[t] = n_useful;
+            p.count_out[p.n + t] = n_slots;
+        }
+    }
+}
+
 template <int OP>
 __global__ void __launch_bounds__(256) tor_kernel(const TorParams p) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t t = warp; t < p.n; t += nwarps) generic_lor<OP>(p, t, lane);
+}
+
+// ---------------------------------------------------------------------------------
+// Fast path: per-LOR constants, per-slice visit, and two kernels built on them.
+//
+// Same traversal and the same float arithmetic for every quantity the reference
+// rounds, with three changes that cut the instruction count per voxel slot:
+//  * the P column offsets dx_i = X_x - mesh_x(i) are computed once per slice;
+//  * rows and columns that cannot hold a voxel inside the cut-off are skipped: over
+//    a row at offset dy the smallest d^2 is dy^2 uz^2/(1 - ux^2) (minimising the
+//    quadratic in dx), over a column dx^2 uz^2/(1 - uy^2); a row/column is skipped
+//    only when that bound exceeds the cut-off with a 0.1 % margin, far above the float
+//    error of d^2, so every voxel the reference weights non-zero is still evaluated
+//    with the exact test;
+//  * the weight is one raw ex2 and the slot test is predicated, not branched.
+
+struct LorConst {
+    float x1, y1, z1, d0, d1, dz, ux, uy;
+    float cut, k1, q_row, q_col, cut_skip;
+    float xc, yc, zc;
+    float scale;
+    int s_lo, s_hi;  // candidate slices (a superset; each is tested exactly)
+};
+
+// Loads LOR t and derives its constants. Returns false when the LOR contributes
+// nothing (no crossing possible, or a back-projection value at/below 1e-7).
+// `generic` is set for a map LOR whose divisor is zero or non-finite.
+template <int OP>
+__device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorConst &L,
+                                            bool &generic) {
+    generic = false;
+    const int64_t o = t * p.stride;
+    const float x1 = __ldg(p.x1 + o), y1 = __ldg(p.y1 + o), z1 = __ldg(p.z1 + o);
+    const float x2 = __ldg(p.x2 + o), y2 = __ldg(p.y2 + o), z2 = __ldg(p.z2 + o);
+    const float f = __ldg(p.f + o);
+    L.scale = p.tof_scale;
+    if (OP == kBack) {
+        const float v = __ldg(p.values + t);
+        if (!((double)v > 1e-7)) return false;  // tor.cu.cc:203
+        L.scale = __fdiv_rn(p.tof_scale, v);
+    } else if (OP == kMap) {
+        L.scale = __fdiv_rn(1.0f, __ldg(p.values + t));  // tor.cu.cc:239, no threshold
+        if (!(fabsf(L.scale) <= 3.0e38f)) {  // w/0 or w/NaN lands on every visited voxel
+            generic = true;
+            return false;
+        }
+    } else if (OP == kAdj) {
+        L.scale = p.tof_scale * __ldg(p.values + t);
+    }
+    L.x1 = x1;
+    L.y1 = y1;
+    L.z1 = z1;
+    L.d0 = __fsub_rn(x2, x1);
+    L.d1 = __fsub_rn(y2, y1);
+    L.dz = __fsub_rn(z2, z1);
+    const float dis =
+        __fsqrt_rn(__fmaf_rn(L.dz, L.dz, __fmaf_rn(L.d0, L.d0, __fmul_rn(L.d1, L.d1))));
+    L.ux = __fdiv_rn(L.d0, dis);
+    L.uy = __fdiv_rn(L.d1, dis);
+    L.cut = p.cut;
+    L.k1 = p.k1;
+    if (p.geo) {
+        const float tsc = __fmul_rn(p.tor_sigma2, f);  // tor.cu.cc:67
+        L.cut = __double2float_ru(9.0 * (double)tsc);
+        const float inv = 0.5f * kLog2e / tsc;
+        L.k1 = (p.tof_on && OP != kMap) ? (p.a_coef - inv) : -inv;
+    }
+    const float uz = L.dz / dis;
+    const float om_x = 1.0f - L.ux * L.ux, om_y = 1.0f - L.uy * L.uy;
+    const bool prune = om_x > 0.01f && om_y > 0.01f;
+    L.q_row = prune ? uz * uz / om_x : 0.0f;
+    L.q_col = prune ? uz * uz / om_y : 0.0f;
+    L.cut_skip = L.cut * 1.001f + 1e-6f;
+    L.xc = L.yc = L.zc = 0.0f;
+    if (OP != kMap && OP != kCount && p.tof_on) {
+        L.xc = __ldg(p.xc + o);
+        L.yc = __ldg(p.yc + o);
+        L.zc = __ldg(p.zc + o);
+    }
+    const float zlo = fminf(z1, z2), zhi = fmaxf(z1, z2);
+    if (!(L.dz != 0.0f && zlo == zlo && zhi == zhi && fabsf(zhi - zlo) <= 3.0e38f)) return false;
+    const float flo = floorf((zlo - p.slice0_f) / p.inter_z) - 2.0f;
+    const float fhi = ceilf((zhi - p.slice0_f) / p.inter_z) + 2.0f;
+    L.s_lo = (int)fmaxf(flo, 0.0f);
+    L.s_hi = (int)fminf(fhi, (float)(p.gz - 1));
+    return L.s_lo <= L.s_hi;
+}
+
+// Candidate slice range of LOR t from its endpoints only (cheap pre-filter).
+__device__ __forceinline__ bool lor_slices(const TorParams &p, int64_t t, int &s_lo,
+                                           int &s_hi) {
+    const int64_t o = t * p.stride;
+    const float z1 = __ldg(p.z1 + o), z2 = __ldg(p.z2 + o);
+    const float zlo = fminf(z1, z2), zhi = fmaxf(z1, z2);
+    if (!(z1 != z2 && zlo == zlo && zhi == zhi && fabsf(zhi - zlo) <= 3.0e38f)) return false;
+    s_lo = (int)fmaxf(floorf((zlo - p.slice0_f) / p.inter_z) - 2.0f, 0.0f);
+    s_hi = (int)fminf(ceilf((zhi - p.slice0_f) / p.inter_z) + 2.0f, (float)(p.gz - 1));
+    return s_lo <= s_hi;
+}
+
+// One (LOR, slice): the reference's crossing test and window (tor.cu.cc:22-48,
+// :135-136), then every voxel with non-zero weight: f(index_in_slice, w) with w the
+// unscaled weight. Returns the number of in-slice window voxels (for kCount).
+template <int OP, int P, typename F>
+__device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L, int s, F &&f) {
+    const float sz = slice_z<OP>(p, s);
+    const float ratio = __fdiv_rn(__fsub_rn(sz, L.z1), L.dz);
+    if (!(ratio > 0.0f && ratio < 1.0f)) return 0;
+    const float cx = __fmaf_rn(L.d0, ratio, L.x1);
+    const float cy = __fmaf_rn(L.d1, ratio, L.y1);
+    const int ix0 = __float2int_rz(__fdiv_rn(__fsub_rn(cx, p.l_bound), p.inter_x)) - p.half;
+    const int iy0 = __float2int_rz(__fdiv_rn(__fsub_rn(cy, p.b_bound), p.inter_y)) - p.half;
+    float k0 = 0.0f;
+    if (OP != kMap && OP != kCount && p.tof_on) {
+        const float ax = __fsub_rn(L.xc, cx), ay = __fsub_rn(L.yc, cy), az = __fsub_rn(L.zc, sz);
+        const float a2 = __fmaf_rn(az, az, __fmaf_rn(ax, ax, __fmul_rn(ay, ay)));
+        k0 = -a2 * p.a_coef;
+    }
+    int n_slots = 0;
+    if (OP == kCount) {
+        const int i_lo = max(0, -ix0), i_hi = min(P, p.gx - ix0);
+        const int j_lo = max(0, -iy0), j_hi = min(P, p.gy - iy0);
+        n_slots = max(0, i_hi - i_lo) * max(0, j_hi - j_lo);
+    }
+    float dxs[P];
+    unsigned colmask = 0u;
+#pragma unroll
+    for (int i = 0; i < P; i++) {
+        const int ix = ix0 + i;
+        const float mx = __fmaf_rn(p.inter_x, (float)ix + 0.5f, p.l_bound);
+        dxs[i] = __fsub_rn(cx, mx);
+        const bool ok = (unsigned)ix < (unsigned)p.gx && dxs[i] * dxs[i] * L.q_col <= L.cut_skip;
+        colmask |= ok ? (1u << i) : 0u;
+    }
+    if (colmask == 0u) return n_slots;
+#pragma unroll
+    for (int j = 0; j < P; j++) {
+        const int iy = iy0 + j;
+        const float my = __fmaf_rn(p.inter_y, (float)iy + 0.5f, p.b_bound);
+        const float dy = __fsub_rn(cy, my);
+        if ((unsigned)iy >= (unsigned)p.gy || dy * dy * L.q_row > L.cut_skip) continue;
+        const float dyuy = __fmul_rn(dy, L.uy);
+        const float dy2 = __fmul_rn(dy, dy);
+        const int row = iy * p.gx + ix0;
+#pragma unroll
+        for (int i = 0; i < P; i++) {
+            const float rc = __fmaf_rn(dxs[i], L.ux, dyuy);
+            const float d2 = __fmaf_rn(-rc, rc, __fmaf_rn(dxs[i], dxs[i], dy2));
+            const bool use = ((colmask >> i) & 1u) && d2 < L.cut;
+            const float w = fast_exp2(fmaf(d2, L.k1, k0));
+            if (use) f(row + i, w);
+        }
+    }
+    return n_slots;
+}
+
+// LOR-centric kernel: one warp per LOR, lanes over its slices; projection gathers
+// from the image in L2/L1, scatter ops use global atomics.
+template <int OP, int P>
+__global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t slice_mesh = (int64_t)p.gx * p.gy;
-
     for (int64_t t = warp; t < p.n; t += nwarps) {
-        const int64_t o = t * p.stride;
-        const float x1 = __ldg(p.x1 + o), y1 = __ldg(p.y1 + o), z1 = __ldg(p.z1 + o);
-        const float x2 = __ldg(p.x2 + o), y2 = __ldg(p.y2 + o), z2 = __ldg(p.z2 + o);
-        const float f = __ldg(p.f + o);
-
-        // Per-LOR output scale and the early-outs of the reference's value tests.
-        float scale = p.tof_scale;
-        bool all_slots = false;  // map with a zero/non-finite divisor: every visited voxel gets w/v
-        if (OP == kBack) {
-            float v = __ldg(p.values + t);
-            if (!((double)v > 1e-7)) continue;  // tor.cu.cc:203
-            scale = __fdiv_rn(p.tof_scale, v);
-        } else if (OP == kMap) {
-            float v = __ldg(p.values + t);
-            scale = __fdiv_rn(1.0f, v);  // tor.cu.cc:239 divides without a threshold
-            all_slots = !(fabsf(scale) <= 3.0e38f);
-        } else if (OP == kAdj) {
-            scale = p.tof_scale * __ldg(p.values + t);
+        LorConst L;
+        bool generic;
+        const bool any = lor_prepare<OP>(p, t, L, generic);
+        if (OP == kMap && generic) {
+            generic_lor<kMap>(p, t, lane);
+            continue;
         }
-
-        const float d0 = __fsub_rn(x2, x1), d1 = __fsub_rn(y2, y1), dz = __fsub_rn(z2, z1);
-        const float dis = __fsqrt_rn(__fmaf_rn(dz, dz, __fmaf_rn(d0, d0, __fmul_rn(d1, d1))));
-        const float ux = __fdiv_rn(d0, dis), uy = __fdiv_rn(d1, dis);
-
-        float cut = p.cut, k1 = p.k1;
-        if (p.geo) {
-            const float tsc = __fmul_rn(p.tor_sigma2, f);  // tor.cu.cc:67
-            cut = __double2float_ru(9.0 * (double)tsc);
-            const float inv = 0.5f * kLog2e / tsc;
-            k1 = (p.tof_on && OP != kMap) ? (p.a_coef - inv) : -inv;
-        }
-
-        // Candidate slices: every s whose plane lies strictly inside (z1, z2), with a
-        // margin; each is then tested with the reference's own ratio.
         float acc = 0.0f;
         int n_useful = 0, n_slots = 0;
-        const float zlo = fminf(z1, z2), zhi = fmaxf(z1, z2);
-        if (dz != 0.0f && zlo == zlo && zhi == zhi && fabsf(zhi - zlo) <= 3.0e38f) {
-            const float flo = floorf((zlo - p.slice0_f) / p.inter_z) - 2.0f;
-            const float fhi = ceilf((zhi - p.slice0_f) / p.inter_z) + 2.0f;
-            const int s_lo = (int)fmaxf(flo, 0.0f);
-            const int s_hi = (int)fminf(fhi, (float)(p.gz - 1));
-            float xc = 0.f, yc = 0.f, zc = 0.f;
-            if (OP != kMap && p.tof_on) {
-                xc = __ldg(p.xc + o);
-                yc = __ldg(p.yc + o);
-                zc = __ldg(p.zc + o);
-            }
-            for (int s = s_lo + lane; s <= s_hi; s += 32) {
-                const float sz = slice_z<OP>(p, s);
-                const float ratio = __fdiv_rn(__fsub_rn(sz, z1), dz);
-                if (!(ratio > 0.0f && ratio < 1.0f)) continue;
-                const float cx = __fmaf_rn(d0, ratio, x1);
-                const float cy = __fmaf_rn(d1, ratio, y1);
-                const int ix0 =
-                    __float2int_rz(__fdiv_rn(__fsub_rn(cx, p.l_bound), p.inter_x)) - p.half;
-                const int iy0 =
-                    __float2int_rz(__fdiv_rn(__fsub_rn(cy, p.b_bound), p.inter_y)) - p.half;
-                float k0 = 0.0f;
-                if (OP != kMap && p.tof_on) {
-                    const float ax = __fsub_rn(xc, cx), ay = __fsub_rn(yc, cy),
-                                az = __fsub_rn(zc, sz);
-                    const float a2 = __fmaf_rn(az, az, __fmaf_rn(ax, ax, __fmul_rn(ay, ay)));
-                    k0 = -a2 * p.a_coef;
-                }
-                const int i_lo = max(0, -ix0), i_hi = min(p.patch, p.gx - ix0);
-                const int j_lo = max(0, -iy0), j_hi = min(p.patch, p.gy - iy0);
-                if (OP == kCount) n_slots += max(0, i_hi - i_lo) * max(0, j_hi - j_lo);
+        if (any) {
+            for (int s = L.s_lo + lane; s <= L.s_hi; s += 32) {
                 const int64_t base = (int64_t)s * slice_mesh;
-                for (int j = j_lo; j < j_hi; ++j) {
-                    const int iy = iy0 + j;
-                    const float my = __fmaf_rn(p.inter_y, (float)iy + 0.5f, p.b_bound);
-                    const float dy = __fsub_rn(cy, my);
-                    const float dyuy = __fmul_rn(dy, uy);
-                    const float dy2 = __fmul_rn(dy, dy);
-                    const int64_t row = base + (int64_t)iy * p.gx;
-                    for (int i = i_lo; i < i_hi; ++i) {
-                        const int ix = ix0 + i;
-                        const float mx = __fmaf_rn(p.inter_x, (float)ix + 0.5f, p.l_bound);
-                        const float dx = __fsub_rn(cx, mx);
-                        const float rc = __fmaf_rn(dx, ux, dyuy);
-                        const float d2 = __fmaf_rn(-rc, rc, __fmaf_rn(dx, dx, dy2));
-                        if (d2 < cut) {
-                            const float w = exp2f(fmaf(d2, k1, k0));
-                            if (OP == kCount) {
-                                n_useful++;
-                            } else if (OP == kProj) {
-                                acc = fmaf(w, __ldg(p.image_in + row + ix), acc);
-                            } else {
-                                atomicAdd(p.image_out + row + ix, w * scale);
-                            }
-                        } else if (OP == kMap && all_slots) {
-                            atomicAdd(p.image_out + row + ix, 0.0f * scale);
-                        }
+                n_slots += slice_visit<OP, P>(p, L, s, [&](int idx, float w) {
+                    if (OP == kCount) {
+                        n_useful++;
+                    } else if (OP == kProj) {
+                        acc = fmaf(w, __ldg(p.image_in + base + idx), acc);
+                    } else {
+                        atomicAdd(p.image_out + base + idx, w * L.scale);
                     }
-                }
+                });
             }
         }
         if (OP == kProj) {
             acc = warp_sum(acc);
-            if (lane == 0) p.proj_out[t] = acc * scale;
+            if (lane == 0) p.proj_out[t] = any ? acc * L.scale : 0.0f;
         }
         if (OP == kCount) {
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                n_useful += __shfl_xor_sync(0xffffffffu, n_useful, o);
-                n_slots += __shfl_xor_sync(0xffffffffu, n_slots, o);
+            for (int o2 = 16; o2 > 0; o2 >>= 1) {
+                n_useful += __shfl_xor_sync(0xffffffffu, n_useful, o2);
+                n_slots += __shfl_xor_sync(0xffffffffu, n_slots, o2);
             }
             if (lane == 0) {
                 p.count_out[t] = n_useful;
                 p.count_out[p.n + t] = n_slots;
             }
         }
+    }
+}
+
+// Slab kernel for the scatter ops (back-projection, map, adjoint). A CTA owns
+// `nsl` consecutive slices [S0, S0+nsl) of the kernel-layout image in shared memory
+// and one contiguous chunk of LORs. Its warps pull LORs whose candidate slice range
+// meets the slab into a per-warp queue (so all 32 lanes work), each lane then walks
+// its LOR's slices inside the slab and accumulates with shared-memory atomics; at the
+// end the slab is added to the output once. Global atomics drop from one per
+// non-zero voxel weight to one per slab voxel per CTA.
+constexpr int kSlabThreads = 512;
+constexpr int kSlabWarps = kSlabThreads / 32;
+
+template <int OP, int P>
+__global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams p, int nsl_max,
+                                                               int n_slabs, int64_t chunk) {
+    extern __shared__ float slab[];
+    __shared__ int queue[kSlabWarps][64];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int k = blockIdx.x % n_slabs;
+    const int64_t c = blockIdx.x / n_slabs;
+    const int S0 = k * nsl_max;
+    const int S1 = min(S0 + nsl_max, p.gz);
+    const int slice_mesh = p.gx * p.gy;
+    const int slab_vox = (S1 - S0) * slice_mesh;
+    for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) slab[i] = 0.0f;
+    __syncthreads();
+
+    const int64_t lo = c * chunk;
+    const int64_t hi = min(p.n, lo + chunk);
+    int pending = 0;
+    auto process = [&](int64_t t) {
+        LorConst L;
+        bool generic;
+        if (!lor_prepare<OP>(p, t, L, generic)) return;
+        const int a = max(L.s_lo, S0), b = min(L.s_hi, S1 - 1);
+        for (int s = a; s <= b; ++s) {
+            const int base = (s - S0) * slice_mesh;
+            slice_visit<OP, P>(p, L, s, [&](int idx, float w) {
+                atomicAdd(&slab[base + idx], w * L.scale);
+            });
+        }
+    };
+    for (int64_t b0 = lo + (int64_t)warp * 32; b0 < hi; b0 += (int64_t)kSlabWarps * 32) {
+        const int64_t t = b0 + lane;
+        bool hit = false;
+        int s_lo, s_hi;
+        if (t < hi && lor_slices(p, t, s_lo, s_hi)) hit = s_hi >= S0 && s_lo < S1;
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit) queue[warp][pending + __popc(m & ((1u << lane) - 1u))] = (int)(t - lo);
+        pending += __popc(m);
+        __syncwarp();
+        if (pending >= 32) {
+            process(lo + queue[warp][lane]);
+            const int rest = pending - 32;
+            const int carry = lane < rest ? queue[warp][32 + lane] : 0;
+            __syncwarp();
+            if (lane < rest) queue[warp][lane] = carry;
+            pending = rest;
+            __syncwarp();
+        }
+    }
+    if (lane < pending) process(lo + queue[warp][lane]);
+    __syncthreads();
+    float *out = p.image_out + (int64_t)S0 * slice_mesh;
+    for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) {
+        const float v = slab[i];
+        if (v != 0.0f) atomicAdd(out + i, v);
     }
 }
 
@@ -227,15 +516,90 @@ int tor_setup(TorParams &p, const int *grid, const float *center, const float *s
                            : 1.0f;
     p.n = n;
     p.stride = lor_stride;
+    // Scatter-kernel selection: the global-atomics kernel by default; SRF_TOR_SCATTER=slab
+    // selects the shared-memory slab kernel (same results; kept selectable so both
+    // paths stay tested while the slab schedule is being balanced).
+    const char *env = std::getenv("SRF_TOR_SCATTER");
+    p.use_slab = (env && env[0] == 's') ? 1 : 0;
     return SRF_OK;
 }
 
+template <int OP, int P>
+void launch_p(const TorParams &p, int grid, int block, cudaStream_t stream) {
+    tor_kernel_p<OP, P><<<grid, block, 0, stream>>>(p);
+}
+
+constexpr size_t kSlabSmemBytes = 220 * 1024;  // of the 227 KB a CTA can opt into
+
+// Slab geometry for the scatter ops: slices per slab, slabs, LOR chunk per CTA.
+// Returns false when one slice does not fit in shared memory.
+bool slab_plan(const TorParams &p, int &nsl, int &n_slabs, int64_t &chunk, int &grid) {
+    const size_t slice_bytes = sizeof(float) * (size_t)p.gx * p.gy;
+    if (slice_bytes > kSlabSmemBytes) return false;
+    nsl = (int)std::min<size_t>(kSlabSmemBytes / slice_bytes, (size_t)p.gz);
+    n_slabs = (p.gz + nsl - 1) / nsl;
+    // about two CTAs per SM in total (one resident at a time), at least 4096 LORs each
+    const int64_t target = 2LL * num_sms();
+    int64_t splits = std::max<int64_t>(1, (target + n_slabs - 1) / n_slabs);
+    chunk = std::max<int64_t>(4096, (p.n + splits - 1) / splits);
+    splits = (p.n + chunk - 1) / chunk;
+    if (chunk > (int64_t)INT32_MAX || splits * n_slabs > (int64_t)INT32_MAX) return false;
+    grid = (int)(splits * n_slabs);
+    return true;
+}
+
+template <int OP, int P>
+int launch_slab(const TorParams &p, cudaStream_t stream) {
+    int nsl, n_slabs, grid;
+    int64_t chunk;
+    if (!slab_plan(p, nsl, n_slabs, chunk, grid)) return -1;
+    const size_t smem = sizeof(float) * (size_t)nsl * p.gx * p.gy;
+    static std::atomic<unsigned long long> attr_set{0};  // per template instance, per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+    if (!(attr_set.load() & (1ull << dev))) {
+        cudaError_t e = cudaFuncSetAttribute(tor_slab_kernel<OP, P>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kSlabSmemBytes);
+        if (e != cudaSuccess) {
+            set_cuda_error(e);
+            return SRF_ERR_CUDA;
+        }
+        attr_set.fetch_or(1ull << dev);
+    }
+    tor_slab_kernel<OP, P><<<grid, kSlabThreads, smem, stream>>>(p, nsl, n_slabs, chunk);
+    return check_launch();
+}
+
 template <int OP>
-int tor_launch(TorParams &p, cudaStream_t stream) {
+int tor_launch(TorParams &p, cudaStream_t stream, bool generic = false) {
     if (p.n == 0) return SRF_OK;
+    if ((OP == kBack || OP == kMap || OP == kAdj) && !generic && p.use_slab) {
+        int st = -1;
+        switch (p.patch) {
+            case 2: st = launch_slab<OP, 2>(p, stream); break;
+            case 3: st = launch_slab<OP, 3>(p, stream); break;
+            case 4: st = launch_slab<OP, 4>(p, stream); break;
+            case 5: st = launch_slab<OP, 5>(p, stream); break;
+            case 6: st = launch_slab<OP, 6>(p, stream); break;
+            case 7: st = launch_slab<OP, 7>(p, stream); break;
+            case 8: st = launch_slab<OP, 8>(p, stream); break;
+            default: break;
+        }
+        if (st >= 0) return st;
+    }
     const int block = 256;
     const int grid = stride_grid(p.n, block / 32, 8);
-    tor_kernel<OP><<<grid, block, 0, stream>>>(p);
+    switch (generic ? 0 : p.patch) {
+        case 2: launch_p<OP, 2>(p, grid, block, stream); break;
+        case 3: launch_p<OP, 3>(p, grid, block, stream); break;
+        case 4: launch_p<OP, 4>(p, grid, block, stream); break;
+        case 5: launch_p<OP, 5>(p, grid, block, stream); break;
+        case 6: launch_p<OP, 6>(p, grid, block, stream); break;
+        case 7: launch_p<OP, 7>(p, grid, block, stream); break;
+        case 8: launch_p<OP, 8>(p, grid, block, stream); break;
+        default: tor_kernel<OP><<<grid, block, 0, stream>>>(p); break;
+    }
     return check_launch();
 }
 

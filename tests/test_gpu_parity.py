@@ -88,9 +88,17 @@ def test_tor_projection(tcase, pname, axis):
     np.testing.assert_array_equal(gpu_nc, gpu)
 
 
+@pytest.fixture(params=["slab", "global"])
+def scatter_kernel(request, monkeypatch):
+    """Back-projection / map / adjoint have two kernels: global atomics (default) and
+    shared-memory slabs (SRF_TOR_SCATTER=slab). Both must agree with the oracle."""
+    monkeypatch.setenv("SRF_TOR_SCATTER", request.param)
+    return request.param
+
+
 @pytest.mark.parametrize("pname", ["tof530_kw10", "tof530_kw4_geo", "notof"])
 @pytest.mark.parametrize("axis", ["x", "y", "z"])
-def test_tor_backprojection(tcase, pname, axis):
+def test_tor_backprojection(tcase, pname, axis, scatter_kernel):
     kw, geo, b, s2 = _tp(pname)
     lors, img, g, c, s = K.tor_axis(tcase, axis)
     pv = O.tor_projection(lors, img, g, c, s, kw, geo, b, s2, mode="f32")
@@ -107,7 +115,7 @@ def test_tor_backprojection(tcase, pname, axis):
 
 
 @pytest.mark.parametrize("geo", [False, True])
-def test_tor_maplors(geo):
+def test_tor_maplors(geo, scatter_kernel):
     mc = K.map_case(n=4000, seed=7, grid=(128, 128, 64), voxel=3.2)
     for axis in "xyz":
         lors7 = np.ascontiguousarray(mc["groups"][axis].T.astype(np.float32))
@@ -124,7 +132,7 @@ def test_tor_maplors(geo):
 
 
 @pytest.mark.parametrize("pname", ["tof530_kw10", "notof"])
-def test_tor_adjoint_identity(tcase, pname):
+def test_tor_adjoint_identity(tcase, pname, scatter_kernel):
     """<A x, y> = <x, A^T y> for the plain adjoint, evaluated in float64 sums."""
     kw, geo, b, s2 = _tp(pname)
     rng = np.random.default_rng(17)
@@ -357,3 +365,22 @@ def test_cpu_tensors_are_rejected():
     with pytest.raises(TypeError):
         ops.tor_projection(torch.zeros(10, 4), torch.zeros(8, 16, 16), [16, 16, 8], [0, 0, 0],
                            [1, 1, 1], 4.0)
+
+
+def test_tor_maplors_zero_divisor_matches_reference(scatter_kernel):
+    """Maplors divides without a threshold (tor.cu.cc:239): a zero divisor puts inf on
+    voxels with non-zero weight and NaN (0/0) on the other visited voxels."""
+    mc = K.map_case(n=600, seed=12, grid=(64, 64, 32), voxel=6.4)
+    lors7 = np.ascontiguousarray(mc["groups"]["x"].T.astype(np.float32))
+    _, g, c, s = P.axis_view(np.zeros(mc["grid"], np.float32), mc["center"], mc["size"], "x")
+    vals = np.ones(lors7.shape[1], np.float32)
+    hits = O.tor_counts(np.ascontiguousarray(lors7), g, c, s, K.KW_CONFIG)[1]
+    vals[int(np.argmax(hits))] = 0.0  # a LOR that does cross the image
+    gpu = host(ops.tor_maplors(cu(np.zeros((g[2], g[1], g[0]), np.float32)), g, c, s,
+                               cu(lors7), cu(vals), K.KW_CONFIG, False, layout="cn"))
+    ref = O.tor_maplors(lors7, vals, g, c, s, K.KW_CONFIG, False, mode="f32", contract=True)
+    np.testing.assert_array_equal(np.isnan(gpu), np.isnan(ref))
+    np.testing.assert_array_equal(np.isinf(gpu), np.isinf(ref))
+    fin = np.isfinite(ref)
+    assert np.isnan(ref).any() and np.isinf(ref).any()
+    assert K.rel_l2(gpu[fin], ref[fin]) <= TOL
