@@ -219,15 +219,14 @@ struct LorConst {
     float xc, yc, zc;
     float scale;
     int s_lo, s_hi;  // candidate slices (a superset; each is tested exactly)
+    bool all;        // map with a zero / non-finite divisor: every window voxel gets w/v
 };
 
 // Loads LOR t and derives its constants. Returns false when the LOR contributes
 // nothing (no crossing possible, or a back-projection value at/below 1e-7).
-// `generic` is set for a map LOR whose divisor is zero or non-finite.
 template <int OP>
-__device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorConst &L,
-                                            bool &generic) {
-    generic = false;
+__device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorConst &L) {
+    L.all = false;
     const int64_t o = t * p.stride;
     const float x1 = __ldg(p.x1 + o), y1 = __ldg(p.y1 + o), z1 = __ldg(p.z1 + o);
     const float x2 = __ldg(p.x2 + o), y2 = __ldg(p.y2 + o), z2 = __ldg(p.z2 + o);
@@ -239,10 +238,7 @@ __device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorCo
         L.scale = __fdiv_rn(p.tof_scale, v);
     } else if (OP == kMap) {
         L.scale = __fdiv_rn(1.0f, __ldg(p.values + t));  // tor.cu.cc:239, no threshold
-        if (!(fabsf(L.scale) <= 3.0e38f)) {  // w/0 or w/NaN lands on every visited voxel
-            generic = true;
-            return false;
-        }
+        L.all = !(fabsf(L.scale) <= 3.0e38f);  // w/0 or w/NaN lands on every visited voxel
     } else if (OP == kAdj) {
         L.scale = p.tof_scale * __ldg(p.values + t);
     }
@@ -266,7 +262,7 @@ __device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorCo
     }
     const float uz = L.dz / dis;
     const float om_x = 1.0f - L.ux * L.ux, om_y = 1.0f - L.uy * L.uy;
-    const bool prune = om_x > 0.01f && om_y > 0.01f;
+    const bool prune = om_x > 0.01f && om_y > 0.01f && !L.all;
     L.q_row = prune ? uz * uz / om_x : 0.0f;
     L.q_col = prune ? uz * uz / om_y : 0.0f;
     L.cut_skip = L.cut * 1.001f + 1e-6f;
@@ -299,7 +295,9 @@ __device__ __forceinline__ bool lor_slices(const TorParams &p, int64_t t, int &s
 
 // One (LOR, slice): the reference's crossing test and window (tor.cu.cc:22-48,
 // :135-136), then every voxel with non-zero weight: f(index_in_slice, w) with w the
-// unscaled weight. Returns the number of in-slice window voxels (for kCount).
+// unscaled weight (for a map LOR with L.all set, every in-slice window voxel, with
+// w = 0 outside the cut-off, as the reference adds 0/0 there). Returns the number of
+// in-slice window voxels (for kCount).
 template <int OP, int P, typename F>
 __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L, int s, F &&f) {
     const float sz = slice_z<OP>(p, s);
@@ -345,8 +343,9 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
         for (int i = 0; i < P; i++) {
             const float rc = __fmaf_rn(dxs[i], L.ux, dyuy);
             const float d2 = __fmaf_rn(-rc, rc, __fmaf_rn(dxs[i], dxs[i], dy2));
-            const bool use = ((colmask >> i) & 1u) && d2 < L.cut;
-            const float w = fast_exp2(fmaf(d2, L.k1, k0));
+            const bool in_cut = d2 < L.cut;
+            const bool use = ((colmask >> i) & 1u) && (in_cut || L.all);
+            const float w = in_cut ? fast_exp2(fmaf(d2, L.k1, k0)) : 0.0f;
             if (use) f(row + i, w);
         }
     }
@@ -363,12 +362,7 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
     const int64_t slice_mesh = (int64_t)p.gx * p.gy;
     for (int64_t t = warp; t < p.n; t += nwarps) {
         LorConst L;
-        bool generic;
-        const bool any = lor_prepare<OP>(p, t, L, generic);
-        if (OP == kMap && generic) {
-            generic_lor<kMap>(p, t, lane);
-            continue;
-        }
+        const bool any = lor_prepare<OP>(p, t, L);
         float acc = 0.0f;
         int n_useful = 0, n_slots = 0;
         if (any) {
@@ -433,8 +427,7 @@ __global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams 
     int pending = 0;
     auto process = [&](int64_t t) {
         LorConst L;
-        bool generic;
-        if (!lor_prepare<OP>(p, t, L, generic)) return;
+        if (!lor_prepare<OP>(p, t, L)) return;
         const int a = max(L.s_lo, S0), b = min(L.s_hi, S1 - 1);
         for (int s = a; s <= b; ++s) {
             const int base = (s - S0) * slice_mesh;
