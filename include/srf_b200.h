@@ -159,6 +159,26 @@ int srf_recon_process(const float *events, int64_t num_events, int64_t event_str
                       double tof_res, float *out, int64_t *group_counts, void *workspace,
                       int64_t workspace_bytes, void *stream);
 
+/* No counterpart in the reference: srf_recon_process for callers that cannot allocate
+ * device memory when they preprocess (a service with a fixed memory budget that forbids
+ * allocations after start-up, or a latency-critical path where cudaMalloc's implicit
+ * device synchronisation is not acceptable). The partition's scratch comes from a
+ * buffer inside the library (a file-scope __device__ array, 8.1 MiB, held by every GPU
+ * that loads the library until exit) instead of a caller workspace; nothing is
+ * allocated. Limits and rules:
+ *   - num_events <= SRF_RECON_PROCESS_NOALLOC_MAX_EVENTS, else SRF_ERR_UNSUPPORTED
+ *     (nothing launched);
+ *   - the first call on a device looks up the buffer's device address
+ *     (cudaGetSymbolAddress) with that device current: make it before any stream
+ *     capture;
+ *   - all calls on a device share the buffer and it keeps the last call's contents
+ *     (no part needs to start at zero); calls that overlap on the GPU race on it, so
+ *     serialise them on one stream.
+ * Same inputs, outputs and results as srf_recon_process. */
+#define SRF_RECON_PROCESS_NOALLOC_MAX_EVENTS 8388608
+int srf_recon_process_noalloc(const float *events, int64_t num_events, int64_t event_stride,
+                              double tof_res, float *out, int64_t *group_counts, void *stream);
+
 /* Replaces map_process, on_tor_lors.py:243-248: lors [N, >=6] -> out [N, 7] rows
  * (p1, p2 with the dominant axis last, sigma2_factor). */
 int srf_map_process(const float *lors, int64_t num_lors, int64_t lor_stride, float *out,

@@ -41,6 +41,7 @@ SIGNATURES = {
     "srf_preprocess_workspace_size": ([_i64], _i64),
     "srf_recon_process": ([_p, _i64, _i64, C.c_double, _p, _p, _p, _i64, _p], _int),
     "srf_map_process": ([_p, _i64, _i64, _p, _p, _p, _i64, _p], _int),
+    "srf_recon_process_noalloc": ([_p, _i64, _i64, C.c_double, _p, _p, _p], _int),
 }
 
 

@@ -16,6 +16,8 @@
 // That is a stable partition into six buckets (axis, swapped), done with a per-tile
 // count, a scan over tiles and a stable scatter (ballot ranks inside each warp).
 
+#include <mutex>
+
 #include "srf_common.cuh"
 
 namespace srf {
@@ -331,4 +333,82 @@ extern "C" int srf_map_process(const float *lors, int64_t num_lors, int64_t lor_
                                int64_t workspace_bytes, void *stream) {
     return preprocess(lors, num_lors, lor_stride, 0, 1.0e4, out, group_counts, workspace,
                       workspace_bytes, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------------
+// recon_process without any allocation.
+//
+// Some callers cannot allocate device memory at the time they preprocess events: an
+// acquisition-side reconstruction service that owns a fixed memory budget and forbids
+// allocations after start-up, or code on a latency-critical path where cudaMalloc's
+// implicit device synchronisation is not acceptable. srf_recon_process needs a scratch
+// workspace for its stable partition; this variant takes that scratch from a buffer
+// that is part of the library itself, a file-scope __device__ array of fixed size.
+//
+// * The buffer holds the workspace for up to SRF_RECON_PROCESS_NOALLOC_MAX_EVENTS events
+//   (8.1 MiB); every GPU that loads the library keeps it until the process exits.
+//   Larger calls are rejected with SRF_ERR_UNSUPPORTED before anything is launched.
+// * Host code cannot use the array's name as a device address, so the first call on
+//   each device (with that device current) asks the runtime for the address with
+//   cudaGetSymbolAddress and caches it; that first call should therefore happen before
+//   any stream capture.
+// * All calls on a device share the one buffer and it keeps the last call's contents.
+//   Nothing in it needs to start at zero: every byte a call reads was written earlier
+//   in the same call. Calls whose kernels overlap on the GPU (concurrent streams, or
+//   several host threads) race on the buffer; serialise them on one stream.
+// * No cudaMalloc, cudaFree or allocating library routine is called.
+
+namespace srf {
+namespace {
+
+constexpr int64_t kNoAllocMaxEvents = SRF_RECON_PROCESS_NOALLOC_MAX_EVENTS;
+constexpr size_t align256c(size_t v) { return (v + 255) & ~(size_t)255; }
+constexpr int64_t kNoAllocTiles = (kNoAllocMaxEvents + kTile - 1) / kTile;
+constexpr size_t kNoAllocScratchBytes =
+    align256c((size_t)kNoAllocMaxEvents) + align256c(sizeof(int) * kNoAllocTiles * kBuckets) +
+    align256c(sizeof(int64_t) * kNoAllocTiles * kBuckets) +
+    align256c(sizeof(int64_t) * (kBuckets + 1));
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (looked up once).
+int noalloc_scratch(void **ptr) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        set_cuda_error(e);
+        return SRF_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return SRF_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_cuda_error(e);
+            return SRF_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = p;
+    }
+    *ptr = g_noalloc_ptr[dev];
+    return SRF_OK;
+}
+
+}  // namespace
+}  // namespace srf
+
+extern "C" int srf_recon_process_noalloc(const float *events, int64_t num_events,
+                                         int64_t event_stride, double tof_res, float *out,
+                                         int64_t *group_counts, void *stream) {
+    if (num_events < 0) return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > kNoAllocMaxEvents) return SRF_ERR_UNSUPPORTED;
+    void *scratch = nullptr;
+    const int st = noalloc_scratch(&scratch);
+    if (st != SRF_OK) return st;
+    return preprocess(events, num_events, event_stride, 1, tof_res, out, group_counts, scratch,
+                      (int64_t)kNoAllocScratchBytes, (cudaStream_t)stream);
 }
