@@ -397,70 +397,271 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
     }
 }
 
-// Slab kernel for the scatter ops (back-projection, map, adjoint). A CTA owns
-// `nsl` consecutive slices [S0, S0+nsl) of the kernel-layout image in shared memory
-// and one contiguous chunk of LORs. Its warps pull LORs whose candidate slice range
-// meets the slab into a per-warp queue (so all 32 lanes work), each lane then walks
-// its LOR's slices inside the slab and accumulates with shared-memory atomics; at the
-// end the slab is added to the output once. Global atomics drop from one per
-// non-zero voxel weight to one per slab voxel per CTA.
-constexpr int kSlabThreads = 512;
-constexpr int kSlabWarps = kSlabThreads / 32;
+// ---------------------------------------------------------------------------------
+// Slab path for the scatter ops (back-projection, map, adjoint).
+//
+// The kernel-layout image is cut into slabs of `nsl` consecutive slices that fit in
+// shared memory. Each LOR is binned into every slab its candidate slice range meets
+// (a segment = (slab, LOR)); the segments are laid out slab by slab. A persistent grid
+// then gives every CTA an equal, contiguous share of that list: the CTA accumulates its
+// segments' voxel weights into the slab with shared-memory atomics and adds the slab to
+// the output once per slab it touched (a share spans one or two slabs). Global atomics
+// drop from one per non-zero voxel weight (5e9 per 10M-event pass) to one per slab voxel
+// per CTA, and no SM waits on an overfull slab.
+//
+// Binning (three kernels, deterministic counts, order inside a slab unspecified):
+//   seg_count  per LOR: slab range -> packed (k_lo, k_hi); per-tile slab histogram
+//   seg_scan   per slab: scan over tiles; slab offsets; total
+//   seg_fill   per LOR: write its index into each slab's list
 
-template <int OP, int P>
-__global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams p, int nsl_max,
-                                                               int n_slabs, int64_t chunk) {
-    extern __shared__ float slab[];
-    __shared__ int queue[kSlabWarps][64];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int k = blockIdx.x % n_slabs;
-    const int64_t c = blockIdx.x / n_slabs;
-    const int S0 = k * nsl_max;
-    const int S1 = min(S0 + nsl_max, p.gz);
-    const int slice_mesh = p.gx * p.gy;
-    const int slab_vox = (S1 - S0) * slice_mesh;
-    for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) slab[i] = 0.0f;
+constexpr int kSegThreads = 512;
+constexpr int kSegItems = 8;
+constexpr int kSegTile = kSegThreads * kSegItems;
+constexpr int kMaxSlabs = 1024;
+constexpr int kSlabThreads = 1024;
+constexpr size_t kSlabSmemBytes = 220 * 1024;  // of the 227 KB a CTA can opt into
+
+struct SegPlan {
+    int nsl, n_slabs, ntiles;
+    int *range;            // [n] packed k_lo | k_hi << 16, or -1
+    int *tile_counts;      // [ntiles * n_slabs]
+    int64_t *tile_offs;    // [ntiles * n_slabs]
+    int64_t *slab_offs;    // [n_slabs + 1]
+    int *seg;              // [capacity] LOR indices, slab-major
+};
+
+template <int OP>
+__global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams p, SegPlan sp) {
+    __shared__ int hist[kMaxSlabs];
+    for (int k = threadIdx.x; k < sp.n_slabs; k += kSegThreads) hist[k] = 0;
     __syncthreads();
-
-    const int64_t lo = c * chunk;
-    const int64_t hi = min(p.n, lo + chunk);
-    int pending = 0;
-    auto process = [&](int64_t t) {
-        LorConst L;
-        if (!lor_prepare<OP>(p, t, L)) return;
-        const int a = max(L.s_lo, S0), b = min(L.s_hi, S1 - 1);
-        for (int s = a; s <= b; ++s) {
-            const int base = (s - S0) * slice_mesh;
-            slice_visit<OP, P>(p, L, s, [&](int idx, float w) {
-                atomicAdd(&slab[base + idx], w * L.scale);
-            });
+    const int64_t base = (int64_t)blockIdx.x * kSegTile;
+    for (int it = 0; it < kSegItems; it++) {
+        const int64_t t = base + (int64_t)it * kSegThreads + threadIdx.x;
+        if (t >= p.n) break;
+        int s_lo, s_hi, packed = -1;
+        bool ok = lor_slices(p, t, s_lo, s_hi);
+        if (ok && OP == kBack) ok = (double)__ldg(p.values + t) > 1e-7;  // tor.cu.cc:203
+        if (ok) {
+            const int k_lo = s_lo / sp.nsl, k_hi = s_hi / sp.nsl;
+            packed = k_lo | (k_hi << 16);
+            for (int k = k_lo; k <= k_hi; k++) atomicAdd(&hist[k], 1);
         }
-    };
-    for (int64_t b0 = lo + (int64_t)warp * 32; b0 < hi; b0 += (int64_t)kSlabWarps * 32) {
-        const int64_t t = b0 + lane;
-        bool hit = false;
-        int s_lo, s_hi;
-        if (t < hi && lor_slices(p, t, s_lo, s_hi)) hit = s_hi >= S0 && s_lo < S1;
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if (hit) queue[warp][pending + __popc(m & ((1u << lane) - 1u))] = (int)(t - lo);
-        pending += __popc(m);
-        __syncwarp();
-        if (pending >= 32) {
-            process(lo + queue[warp][lane]);
-            const int rest = pending - 32;
-            const int carry = lane < rest ? queue[warp][32 + lane] : 0;
-            __syncwarp();
-            if (lane < rest) queue[warp][lane] = carry;
-            pending = rest;
-            __syncwarp();
+        sp.range[t] = packed;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < sp.n_slabs; k += kSegThreads)
+        sp.tile_counts[(int64_t)blockIdx.x * sp.n_slabs + k] = hist[k];
+}
+
+// Per slab (one block each): exclusive scan of the tile counts -> tile_offs, slab total
+// -> slab_tot[k]. A second single-warp kernel turns the totals into slab offsets.
+__global__ void __launch_bounds__(1024) seg_scan_kernel(SegPlan sp, int64_t *slab_tot) {
+    __shared__ int64_t warp_sums[32];
+    const int k = blockIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int64_t carry = 0;
+    for (int start = 0; start < sp.ntiles; start += 1024) {
+        const int tile = start + threadIdx.x;
+        const int64_t v = tile < sp.ntiles ? sp.tile_counts[(int64_t)tile * sp.n_slabs + k] : 0;
+        int64_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int64_t w = warp_sums[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        const int64_t before = (wid ? warp_sums[wid - 1] : 0) + carry;
+        if (tile < sp.ntiles) sp.tile_offs[(int64_t)tile * sp.n_slabs + k] = before + x - v;
+        const int64_t chunk = warp_sums[31];
+        __syncthreads();
+        carry += chunk;
+    }
+    if (threadIdx.x == 0) slab_tot[k] = carry;
+}
+
+__global__ void seg_offsets_kernel(SegPlan sp, const int64_t *slab_tot) {
+    if (threadIdx.x == 0) {
+        int64_t acc = 0;
+        for (int k = 0; k < sp.n_slabs; k++) {
+            sp.slab_offs[k] = acc;
+            acc += slab_tot[k];
+        }
+        sp.slab_offs[sp.n_slabs] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p, SegPlan sp) {
+    __shared__ int cursor[kMaxSlabs];
+    for (int k = threadIdx.x; k < sp.n_slabs; k += kSegThreads) cursor[k] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSegTile;
+    for (int it = 0; it < kSegItems; it++) {
+        const int64_t t = base + (int64_t)it * kSegThreads + threadIdx.x;
+        if (t >= p.n) break;
+        const int packed = sp.range[t];
+        if (packed < 0) continue;
+        const int k_lo = packed & 0xffff, k_hi = packed >> 16;
+        for (int k = k_lo; k <= k_hi; k++) {
+            const int pos = atomicAdd(&cursor[k], 1);
+            sp.seg[sp.slab_offs[k] + sp.tile_offs[(int64_t)blockIdx.x * sp.n_slabs + k] + pos] =
+                (int)t;
         }
     }
-    if (lane < pending) process(lo + queue[warp][lane]);
-    __syncthreads();
-    float *out = p.image_out + (int64_t)S0 * slice_mesh;
-    for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) {
-        const float v = slab[i];
-        if (v != 0.0f) atomicAdd(out + i, v);
+}
+
+// Persistent pass over the slab-major segment list (all TOR ops but the count).
+// Each warp takes 32 segments, expands them into (segment, slice) items and hands out
+// 32 items per round, so every lane walks one slice of one LOR; the LOR constants come
+// from the segment's lane by shuffle. Scatter ops accumulate into the slab with shared
+// atomics and flush once per slab; the projection gathers from the slab (loaded from
+// the image) and adds each LOR's partial sum, reduced across the warp, to its output.
+template <int OP>
+__device__ __forceinline__ LorConst shfl_lor(const LorConst &L, int src) {
+    LorConst M;
+    M.x1 = __shfl_sync(0xffffffffu, L.x1, src);
+    M.y1 = __shfl_sync(0xffffffffu, L.y1, src);
+    M.z1 = __shfl_sync(0xffffffffu, L.z1, src);
+    M.d0 = __shfl_sync(0xffffffffu, L.d0, src);
+    M.d1 = __shfl_sync(0xffffffffu, L.d1, src);
+    M.dz = __shfl_sync(0xffffffffu, L.dz, src);
+    M.ux = __shfl_sync(0xffffffffu, L.ux, src);
+    M.uy = __shfl_sync(0xffffffffu, L.uy, src);
+    M.cut = __shfl_sync(0xffffffffu, L.cut, src);
+    M.k1 = __shfl_sync(0xffffffffu, L.k1, src);
+    M.q_row = __shfl_sync(0xffffffffu, L.q_row, src);
+    M.q_col = __shfl_sync(0xffffffffu, L.q_col, src);
+    M.cut_skip = __shfl_sync(0xffffffffu, L.cut_skip, src);
+    if (OP != kMap) {
+        M.xc = __shfl_sync(0xffffffffu, L.xc, src);
+        M.yc = __shfl_sync(0xffffffffu, L.yc, src);
+        M.zc = __shfl_sync(0xffffffffu, L.zc, src);
+    } else {
+        M.xc = M.yc = M.zc = 0.0f;
+    }
+    M.scale = __shfl_sync(0xffffffffu, L.scale, src);
+    M.all = OP == kMap ? (bool)__shfl_sync(0xffffffffu, (int)L.all, src) : false;
+    M.s_lo = M.s_hi = 0;
+    return M;
+}
+
+template <int OP, int P>
+__global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams p, SegPlan sp) {
+    extern __shared__ float slab[];
+    __shared__ signed char owner_tab[kSlabThreads / 32][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int kWarps = kSlabThreads / 32;
+    const int slice_mesh = p.gx * p.gy;
+    const int64_t total = sp.slab_offs[sp.n_slabs];
+    const int64_t g = blockIdx.x, G = gridDim.x;
+    const int64_t lo = total * g / G, hi = total * (g + 1) / G;
+    if (lo >= hi) return;
+    int k = 0;
+    {
+        int a = 0, b = sp.n_slabs - 1;
+        while (a < b) {
+            const int m = (a + b + 1) >> 1;
+            if (sp.slab_offs[m] <= lo) a = m; else b = m - 1;
+        }
+        k = a;
+    }
+    int64_t pos = lo;
+    while (pos < hi) {
+        while (sp.slab_offs[k + 1] <= pos) k++;  // skip empty slabs
+        const int64_t end = min(hi, sp.slab_offs[k + 1]);
+        const int S0 = k * sp.nsl;
+        const int S1 = min(S0 + sp.nsl, p.gz);
+        const int slab_vox = (S1 - S0) * slice_mesh;
+        if (OP == kProj) {
+            const float *src = p.image_in + (int64_t)S0 * slice_mesh;
+            for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) slab[i] = __ldg(src + i);
+        } else {
+            for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) slab[i] = 0.0f;
+        }
+        __syncthreads();
+        for (int64_t q0 = pos + (int64_t)warp * 32; q0 < end; q0 += (int64_t)kWarps * 32) {
+            const int64_t q = q0 + lane;
+            LorConst L;
+            int a = 0, cnt = 0, t = -1;
+            if (q < end) {
+                t = sp.seg[q];
+                if (lor_prepare<OP>(p, t, L)) {
+                    a = max(L.s_lo, S0);
+                    cnt = max(0, min(L.s_hi, S1 - 1) - a + 1);
+                }
+            }
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int excl = incl - cnt;
+            const int n_items = __shfl_sync(0xffffffffu, incl, 31);
+            for (int base = 0; base < n_items; base += 32) {
+                for (int i = max(excl, base); i < min(incl, base + 32); ++i)
+                    owner_tab[warp][i - base] = (signed char)lane;
+                __syncwarp();
+                const int item = base + lane;
+                const bool valid = item < n_items;
+                const int o = valid ? (int)owner_tab[warp][lane] : 0;
+                __syncwarp();
+                const LorConst M = shfl_lor<OP>(L, o);
+                const int a_o = __shfl_sync(0xffffffffu, a, o);
+                const int excl_o = __shfl_sync(0xffffffffu, excl, o);
+                const int t_o = __shfl_sync(0xffffffffu, t, o);
+                float partial = 0.0f;
+                if (valid) {
+                    const int s = a_o + (item - excl_o);
+                    const int off = (s - S0) * slice_mesh;
+                    if (OP == kProj) {
+                        float acc = 0.0f;
+                        slice_visit<OP, P>(p, M, s, [&](int idx, float w) {
+                            acc = fmaf(w, slab[off + idx], acc);
+                        });
+                        partial = acc * M.scale;
+                    } else {
+                        slice_visit<OP, P>(p, M, s, [&](int idx, float w) {
+                            atomicAdd(&slab[off + idx], w * M.scale);
+                        });
+                    }
+                }
+                if (OP == kProj) {
+                    // items of one LOR sit in consecutive lanes: segmented suffix sum
+                    const int key = valid ? o : -1 - lane;
+                    float v = partial;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const float nv = __shfl_down_sync(0xffffffffu, v, d);
+                        const int nk = __shfl_down_sync(0xffffffffu, key, d);
+                        if (lane + d < 32 && nk == key) v += nv;
+                    }
+                    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+                    if (valid && (lane == 0 || prev != key)) atomicAdd(p.proj_out + t_o, v);
+                }
+            }
+        }
+        __syncthreads();
+        if (OP != kProj) {
+            float *out = p.image_out + (int64_t)S0 * slice_mesh;
+            for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) {
+                const float v = slab[i];
+                if (v != 0.0f) atomicAdd(out + i, v);
+            }
+            __syncthreads();
+        }
+        pos = end;
     }
 }
 
@@ -509,11 +710,11 @@ int tor_setup(TorParams &p, const int *grid, const float *center, const float *s
                            : 1.0f;
     p.n = n;
     p.stride = lor_stride;
-    // Scatter-kernel selection: the global-atomics kernel by default; SRF_TOR_SCATTER=slab
-    // selects the shared-memory slab kernel (same results; kept selectable so both
-    // paths stay tested while the slab schedule is being balanced).
+    // Kernel selection: the shared-memory slab kernels by default (when a slice fits in
+    // shared memory); SRF_TOR_SCATTER=global selects the LOR-centric kernels (gathers from
+    // L2, global atomics), the fallback for larger slices, so that tests exercise both.
     const char *env = std::getenv("SRF_TOR_SCATTER");
-    p.use_slab = (env && env[0] == 's') ? 1 : 0;
+    p.use_slab = (env && env[0] == 'g') ? 0 : 1;
     return SRF_OK;
 }
 
@@ -522,52 +723,86 @@ void launch_p(const TorParams &p, int grid, int block, cudaStream_t stream) {
     tor_kernel_p<OP, P><<<grid, block, 0, stream>>>(p);
 }
 
-constexpr size_t kSlabSmemBytes = 220 * 1024;  // of the 227 KB a CTA can opt into
-
-// Slab geometry for the scatter ops: slices per slab, slabs, LOR chunk per CTA.
-// Returns false when one slice does not fit in shared memory.
-bool slab_plan(const TorParams &p, int &nsl, int &n_slabs, int64_t &chunk, int &grid) {
+// Slices per slab (as many as fit in shared memory) and slab count; false when one
+// slice does not fit (the global-atomics kernel is used then).
+bool slab_geometry(const TorParams &p, int &nsl, int &n_slabs) {
     const size_t slice_bytes = sizeof(float) * (size_t)p.gx * p.gy;
     if (slice_bytes > kSlabSmemBytes) return false;
     nsl = (int)std::min<size_t>(kSlabSmemBytes / slice_bytes, (size_t)p.gz);
     n_slabs = (p.gz + nsl - 1) / nsl;
-    // about two CTAs per SM in total (one resident at a time), at least 4096 LORs each
-    const int64_t target = 2LL * num_sms();
-    int64_t splits = std::max<int64_t>(1, (target + n_slabs - 1) / n_slabs);
-    chunk = std::max<int64_t>(4096, (p.n + splits - 1) / splits);
-    splits = (p.n + chunk - 1) / chunk;
-    if (chunk > (int64_t)INT32_MAX || splits * n_slabs > (int64_t)INT32_MAX) return false;
-    grid = (int)(splits * n_slabs);
-    return true;
+    return n_slabs <= kMaxSlabs && p.n < (int64_t)INT32_MAX;
 }
 
 template <int OP, int P>
 int launch_slab(const TorParams &p, cudaStream_t stream) {
-    int nsl, n_slabs, grid;
-    int64_t chunk;
-    if (!slab_plan(p, nsl, n_slabs, chunk, grid)) return -1;
-    const size_t smem = sizeof(float) * (size_t)nsl * p.gx * p.gy;
+    SegPlan sp{};
+    if (!slab_geometry(p, sp.nsl, sp.n_slabs)) return -1;
+    sp.ntiles = (int)((p.n + kSegTile - 1) / kSegTile);
+    // Scratch from the stream-ordered pool: no host synchronisation, capturable. The
+    // segment list is sized for the worst case (every LOR in every slab it can reach).
+    const int64_t max_slabs_per_lor = sp.n_slabs;
+    const size_t cap = (size_t)p.n * (size_t)max_slabs_per_lor;
+    auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    const size_t b_range = al(sizeof(int) * p.n);
+    const size_t b_counts = al(sizeof(int) * (size_t)sp.ntiles * sp.n_slabs);
+    const size_t b_offs = al(sizeof(int64_t) * (size_t)sp.ntiles * sp.n_slabs);
+    const size_t b_slab = al(sizeof(int64_t) * (2 * sp.n_slabs + 1));
+    const size_t b_seg = al(sizeof(int) * cap);
+    char *ws = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&ws, b_range + b_counts + b_offs + b_slab + b_seg,
+                                    stream);
+    if (e != cudaSuccess) {
+        set_cuda_error(e);
+        return SRF_ERR_CUDA;
+    }
+    sp.range = reinterpret_cast<int *>(ws);
+    sp.tile_counts = reinterpret_cast<int *>(ws + b_range);
+    sp.tile_offs = reinterpret_cast<int64_t *>(ws + b_range + b_counts);
+    sp.slab_offs = reinterpret_cast<int64_t *>(ws + b_range + b_counts + b_offs);
+    sp.seg = reinterpret_cast<int *>(ws + b_range + b_counts + b_offs + b_slab);
+
     static std::atomic<unsigned long long> attr_set{0};  // per template instance, per device
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
     if (!(attr_set.load() & (1ull << dev))) {
-        cudaError_t e = cudaFuncSetAttribute(tor_slab_kernel<OP, P>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kSlabSmemBytes);
+        e = cudaFuncSetAttribute(tor_slab_kernel<OP, P>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSlabSmemBytes);
         if (e != cudaSuccess) {
             set_cuda_error(e);
+            cudaFreeAsync(ws, stream);
             return SRF_ERR_CUDA;
         }
         attr_set.fetch_or(1ull << dev);
     }
-    tor_slab_kernel<OP, P><<<grid, kSlabThreads, smem, stream>>>(p, nsl, n_slabs, chunk);
-    return check_launch();
+    const size_t smem = sizeof(float) * (size_t)sp.nsl * p.gx * p.gy;
+    int64_t *slab_tot = sp.slab_offs + sp.n_slabs + 1;
+    if (OP == kProj) {
+        e = cudaMemsetAsync(p.proj_out, 0, sizeof(float) * p.n, stream);
+        if (e != cudaSuccess) {
+            set_cuda_error(e);
+            cudaFreeAsync(ws, stream);
+            return SRF_ERR_CUDA;
+        }
+    }
+    seg_count_kernel<OP><<<sp.ntiles, kSegThreads, 0, stream>>>(p, sp);
+    seg_scan_kernel<<<sp.n_slabs, 1024, 0, stream>>>(sp, slab_tot);
+    seg_offsets_kernel<<<1, 32, 0, stream>>>(sp, slab_tot);
+    seg_fill_kernel<<<sp.ntiles, kSegThreads, 0, stream>>>(p, sp);
+    tor_slab_kernel<OP, P><<<num_sms(), kSlabThreads, smem, stream>>>(p, sp);
+    int st = check_launch();
+    e = cudaFreeAsync(ws, stream);
+    if (st == SRF_OK && e != cudaSuccess) {
+        set_cuda_error(e);
+        st = SRF_ERR_CUDA;
+    }
+    return st;
 }
 
 template <int OP>
 int tor_launch(TorParams &p, cudaStream_t stream, bool generic = false) {
     if (p.n == 0) return SRF_OK;
-    if ((OP == kBack || OP == kMap || OP == kAdj) && !generic && p.use_slab) {
+    if ((OP == kProj || OP == kBack || OP == kMap || OP == kAdj) && !generic && p.use_slab) {
         int st = -1;
         switch (p.patch) {
             case 2: st = launch_slab<OP, 2>(p, stream); break;

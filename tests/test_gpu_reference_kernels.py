@@ -31,9 +31,15 @@ def tcase():
     return K.tor_case(n=20000, seed=51, grid=(128, 128, 64), voxel=3.2, n_box=2000)
 
 
+@pytest.fixture(params=["slab", "global"])
+def tor_path(request, monkeypatch):
+    monkeypatch.setenv("SRF_TOR_SCATTER", request.param)
+    return request.param
+
+
 @pytest.mark.parametrize("kw,geo", [(K.KW_CONFIG, False), (4.0, True)])
 @pytest.mark.parametrize("axis", ["x", "y", "z"])
-def test_tor_against_reference_gpu(refgpu, tcase, kw, geo, axis):
+def test_tor_against_reference_gpu(refgpu, tcase, kw, geo, axis, tor_path):
     b, s2 = K.tof_params(530.0)
     lors, img, g, c, s = K.tor_axis(tcase, axis)
     L, I = cu(lors), cu(img)
@@ -42,7 +48,7 @@ def test_tor_against_reference_gpu(refgpu, tcase, kw, geo, axis):
     e = K.rel_l2(got, ref)
     exact = float(np.mean(got == ref))
     record("tor_vs_reference_gpu", kw=kw, geo=geo, axis=axis, n=int(lors.shape[1]), rel_l2=e,
-           bit_equal_fraction=exact)
+           bit_equal_fraction=exact, path=tor_path)
     assert e <= TOL, e
     pv = ref.copy()
     pv[::13] = 0.0
