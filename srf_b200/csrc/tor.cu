@@ -294,7 +294,7 @@ __device__ __forceinline__ bool lor_slices(const TorParams &p, int64_t t, int &s
 }
 
 // One (LOR, slice): the reference's crossing test and window (tor.cu.cc:22-48,
-// :135-136), then every voxel with non-zero weight: f(index_in_slice, w) with w the
+// :135-136), then every voxel with non-zero weight: f(index_in_slice, row, w) with w the
 // unscaled weight (for a map LOR with L.all set, every in-slice window voxel, with
 // w = 0 outside the cut-off, as the reference adds 0/0 there). Returns the number of
 // in-slice window voxels (for kCount).
@@ -346,7 +346,7 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
             const bool in_cut = d2 < L.cut;
             const bool use = ((colmask >> i) & 1u) && (in_cut || L.all);
             const float w = in_cut ? fast_exp2(fmaf(d2, L.k1, k0)) : 0.0f;
-            if (use) f(row + i, w);
+            if (use) f(row + i, iy, w);
         }
     }
     return n_slots;
@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
         if (any) {
             for (int s = L.s_lo + lane; s <= L.s_hi; s += 32) {
                 const int64_t base = (int64_t)s * slice_mesh;
-                n_slots += slice_visit<OP, P>(p, L, s, [&](int idx, float w) {
+                n_slots += slice_visit<OP, P>(p, L, s, [&](int idx, int, float w) {
                     if (OP == kCount) {
                         n_useful++;
                     } else if (OP == kProj) {
@@ -556,6 +556,15 @@ __device__ __forceinline__ LorConst shfl_lor(const LorConst &L, int src) {
     return M;
 }
 
+// Shared-memory slab layout: rows padded to gx + 1 floats and slices to a stride that
+// is 5 (mod 32) floats, so that a warp's lanes — often consecutive slices of one LOR at
+// the same (row, column), or different LORs in one row — fall into different banks.
+__host__ __device__ __forceinline__ int slab_row_stride(int gx) { return gx + 1; }
+__host__ __device__ __forceinline__ int slab_slice_stride(int gx, int gy) {
+    const int dense = gy * (gx + 1);
+    return dense + ((5 - dense % 32) + 32) % 32;
+}
+
 template <int OP, int P>
 __global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams p, SegPlan sp) {
     extern __shared__ float slab[];
@@ -563,6 +572,7 @@ __global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int kWarps = kSlabThreads / 32;
     const int slice_mesh = p.gx * p.gy;
+    const int rs = slab_row_stride(p.gx), ss = slab_slice_stride(p.gx, p.gy);
     const int64_t total = sp.slab_offs[sp.n_slabs];
     const int64_t g = blockIdx.x, G = gridDim.x;
     const int64_t lo = total * g / G, hi = total * (g + 1) / G;
@@ -582,12 +592,17 @@ __global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams 
         const int64_t end = min(hi, sp.slab_offs[k + 1]);
         const int S0 = k * sp.nsl;
         const int S1 = min(S0 + sp.nsl, p.gz);
-        const int slab_vox = (S1 - S0) * slice_mesh;
+        const int n_rows = (S1 - S0) * p.gy;
         if (OP == kProj) {
             const float *src = p.image_in + (int64_t)S0 * slice_mesh;
-            for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) slab[i] = __ldg(src + i);
+            for (int r = warp; r < n_rows; r += kWarps) {
+                const int sl = r / p.gy, iy = r - sl * p.gy;
+                const float *g = src + (int64_t)r * p.gx;
+                float *d = slab + sl * ss + iy * rs;
+                for (int ix = lane; ix < p.gx; ix += 32) d[ix] = __ldg(g + ix);
+            }
         } else {
-            for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) slab[i] = 0.0f;
+            for (int i = threadIdx.x; i < (S1 - S0) * ss; i += kSlabThreads) slab[i] = 0.0f;
         }
         __syncthreads();
         for (int64_t q0 = pos + (int64_t)warp * 32; q0 < end; q0 += (int64_t)kWarps * 32) {
@@ -624,16 +639,16 @@ __global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams 
                 float partial = 0.0f;
                 if (valid) {
                     const int s = a_o + (item - excl_o);
-                    const int off = (s - S0) * slice_mesh;
+                    const int off = (s - S0) * ss;
                     if (OP == kProj) {
                         float acc = 0.0f;
-                        slice_visit<OP, P>(p, M, s, [&](int idx, float w) {
-                            acc = fmaf(w, slab[off + idx], acc);
+                        slice_visit<OP, P>(p, M, s, [&](int idx, int iy, float w) {
+                            acc = fmaf(w, slab[off + idx + iy], acc);
                         });
                         partial = acc * M.scale;
                     } else {
-                        slice_visit<OP, P>(p, M, s, [&](int idx, float w) {
-                            atomicAdd(&slab[off + idx], w * M.scale);
+                        slice_visit<OP, P>(p, M, s, [&](int idx, int iy, float w) {
+                            atomicAdd(&slab[off + idx + iy], w * M.scale);
                         });
                     }
                 }
@@ -655,9 +670,14 @@ __global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams 
         __syncthreads();
         if (OP != kProj) {
             float *out = p.image_out + (int64_t)S0 * slice_mesh;
-            for (int i = threadIdx.x; i < slab_vox; i += kSlabThreads) {
-                const float v = slab[i];
-                if (v != 0.0f) atomicAdd(out + i, v);
+            for (int r = warp; r < n_rows; r += kWarps) {
+                const int sl = r / p.gy, iy = r - sl * p.gy;
+                const float *src = slab + sl * ss + iy * rs;
+                float *g = out + (int64_t)r * p.gx;
+                for (int ix = lane; ix < p.gx; ix += 32) {
+                    const float v = src[ix];
+                    if (v != 0.0f) atomicAdd(g + ix, v);
+                }
             }
             __syncthreads();
         }
@@ -726,7 +746,8 @@ void launch_p(const TorParams &p, int grid, int block, cudaStream_t stream) {
 // Slices per slab (as many as fit in shared memory) and slab count; false when one
 // slice does not fit (the global-atomics kernel is used then).
 bool slab_geometry(const TorParams &p, int &nsl, int &n_slabs) {
-    const size_t slice_bytes = sizeof(float) * (size_t)p.gx * p.gy;
+    if (p.gx > (1 << 15) || p.gy > (1 << 15)) return false;
+    const size_t slice_bytes = sizeof(float) * (size_t)slab_slice_stride(p.gx, p.gy);
     if (slice_bytes > kSlabSmemBytes) return false;
     nsl = (int)std::min<size_t>(kSlabSmemBytes / slice_bytes, (size_t)p.gz);
     n_slabs = (p.gz + nsl - 1) / nsl;
@@ -775,7 +796,7 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
         }
         attr_set.fetch_or(1ull << dev);
     }
-    const size_t smem = sizeof(float) * (size_t)sp.nsl * p.gx * p.gy;
+    const size_t smem = sizeof(float) * (size_t)sp.nsl * slab_slice_stride(p.gx, p.gy);
     int64_t *slab_tot = sp.slab_offs + sp.n_slabs + 1;
     if (OP == kProj) {
         e = cudaMemsetAsync(p.proj_out, 0, sizeof(float) * p.n, stream);
