@@ -100,6 +100,48 @@ int srf_tor_count_samples(const float *x1, const float *y1, const float *z1, con
                           const float *size, float kernel_width, int *counts,
                           int64_t num_events, int64_t lor_stride, void *stream);
 
+/* No counterpart in the reference: batched TOR for many reconstructions that share one
+ * geometry (dynamic frames, many phantoms). LOR i belongs to frame frame[i] (DEVICE
+ * int32[N], 0 <= frame[i] < n_frames); images are n_frames consecutive blocks of
+ * frame_stride floats (>= grid voxels). One launch covers every frame. Semantics per
+ * frame are those of srf_tor_projection / srf_tor_backprojection /
+ * srf_tor_backproject_adjoint; `accumulate` = 0 zeroes all n_frames blocks first. */
+int srf_tor_projection_batched(const float *x1, const float *y1, const float *z1,
+                               const float *x2, const float *y2, const float *z2,
+                               const float *xc, const float *yc, const float *zc,
+                               const float *sigma2_factor, int geo_sigma2_flag,
+                               const int *frame, int n_frames, int64_t frame_stride,
+                               float *projection_value, const int *grid, const float *center,
+                               const float *size, float kernel_width, float tof_bin,
+                               float tof_sigma2, const float *images, int64_t num_events,
+                               int64_t lor_stride, void *stream);
+int srf_tor_backprojection_batched(const float *x1, const float *y1, const float *z1,
+                                   const float *x2, const float *y2, const float *z2,
+                                   const float *xc, const float *yc, const float *zc,
+                                   const float *sigma2_factor, int geo_sigma2_flag,
+                                   const int *frame, int n_frames, int64_t frame_stride,
+                                   const float *projection_value, const int *grid,
+                                   const float *center, const float *size, float kernel_width,
+                                   float tof_bin, float tof_sigma2, float *images,
+                                   int64_t num_events, int64_t lor_stride, int accumulate,
+                                   void *stream);
+int srf_tor_backproject_adjoint_batched(const float *x1, const float *y1, const float *z1,
+                                        const float *x2, const float *y2, const float *z2,
+                                        const float *xc, const float *yc, const float *zc,
+                                        const float *sigma2_factor, int geo_sigma2_flag,
+                                        const int *frame, int n_frames, int64_t frame_stride,
+                                        const float *values, const int *grid,
+                                        const float *center, const float *size,
+                                        float kernel_width, float tof_bin, float tof_sigma2,
+                                        float *images, int64_t num_events, int64_t lor_stride,
+                                        int accumulate, void *stream);
+
+/* No counterpart in the reference: process-wide tuning of the TOR kernels (used by the
+ * autotuner; affects later calls from every thread). path: 0 automatic, 1 shared-memory
+ * slab kernels, 2 LOR-centric kernels (L2 gathers, global atomics); slab_slices: slices
+ * per slab, 0 = as many as fit; grid_mult: persistent slab CTAs = SMs x grid_mult (1..8). */
+int srf_tor_set_tuning(int path, int slab_slices, int grid_mult);
+
 /* ---------------------------------------------------------------------------------- Siddon
  * Field columns for Siddon: x1,y1,z1,x2,y2,z2,tof (tof in mm along the LOR, the
  * reference's convention, siddon.cu.cc:460). Weight 1/L^2 (siddon.cu.cc:459). TOF on

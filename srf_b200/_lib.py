@@ -36,6 +36,14 @@ SIGNATURES = {
     "srf_siddon_maplors": ([_p] * 6 + [_p, _p, _p, _p, _p, _i64, _i64, _int, _p], _int),
     "srf_siddon_backproject_adjoint": (_SID_COLS + [_p, _p, _p, _p, _f, _f, _p, _i64, _i64,
                                                     _int, _p], _int),
+    "srf_tor_projection_batched": (_TOR_COLS + [_int, _p, _int, _i64, _p, _p, _p, _p, _f, _f, _f,
+                                                _p, _i64, _i64, _p], _int),
+    "srf_tor_backprojection_batched": (_TOR_COLS + [_int, _p, _int, _i64, _p, _p, _p, _p, _f, _f,
+                                                    _f, _p, _i64, _i64, _int, _p], _int),
+    "srf_tor_backproject_adjoint_batched": (_TOR_COLS + [_int, _p, _int, _i64, _p, _p, _p, _p,
+                                                         _f, _f, _f, _p, _i64, _i64, _int, _p],
+                                            _int),
+    "srf_tor_set_tuning": ([_int, _int, _int], _int),
     "srf_tor_count_samples": ([_p] * 7 + [_int, _p, _p, _p, _f, _p, _i64, _i64, _p], _int),
     "srf_mlem_update": ([_p, _p, _p, _i64, _p], _int),
     "srf_preprocess_workspace_size": ([_i64], _i64),

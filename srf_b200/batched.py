@@ -1,0 +1,134 @@
+"""Batched OSEM: many independent TOR reconstructions that share one scanner and image
+geometry (dynamic frames, many phantoms) advanced together.
+
+There is no counterpart in the reference, which reconstructs one list at a time
+(``LocalReconstructionGraph``, src/python/srf/graph/reconstruction/local_reconstruction.py).
+Per frame the arithmetic is exactly ``srf_b200.recon.OSEM``'s (the same subsets, the
+same reference back-projection A^T(1/Ax), the same update); what changes is the launch
+structure: the LORs of every frame are concatenated per dominant axis with a frame
+index, the images are stacked [F, nx, ny, nz], and each subset is one batched
+projection and one batched back-projection per axis group for ALL frames — one
+persistent launch per kernel instead of one per frame, with the work balanced across
+SMs over the frames' combined segments. An iteration can be captured in a CUDA graph.
+"""
+
+import torch
+
+from . import ops
+from .data import Image
+from .physics import SplitLoRsModel
+
+
+class FrameBatch:
+    """Per-axis concatenation of several frames' preprocessed LOR records.
+
+    ``frames``: list of dicts {'x','y','z'} -> [N_f_a, 10] CUDA tensors (the output of
+    ``recon_process`` per frame). Subset k of every frame holds its events k, k+S, ...
+    of each axis group (the interleaving of ``srf_b200.recon.make_subsets``)."""
+
+    def __init__(self, frames, n_subsets=1):
+        self.n_frames = len(frames)
+        self.n_subsets = int(n_subsets)
+        self.subsets = []
+        for k in range(self.n_subsets):
+            per_axis = {}
+            for a in SplitLoRsModel.AXIS:
+                parts, ids = [], []
+                for f, g in enumerate(frames):
+                    sub = g[a][k::self.n_subsets] if self.n_subsets > 1 else g[a]
+                    parts.append(sub)
+                    ids.append(torch.full((sub.shape[0],), f, dtype=torch.int32,
+                                          device=sub.device))
+                lors = torch.cat(parts, 0).contiguous()
+                frame = torch.cat(ids, 0).contiguous()
+                per_axis[a] = (lors, frame)
+            self.subsets.append(per_axis)
+
+    def n_lors(self):
+        return sum(l.shape[0] for s in self.subsets for (l, _) in s.values())
+
+
+def _stacked_perm(perm):
+    return [0] + [d + 1 for d in perm]
+
+
+class BatchedOSEM:
+    """OSEM of ``F`` frames at once (TOR model).
+
+    ``model``: SplitLoRsModel; ``frames``: list of per-frame recon_process outputs;
+    ``effinv``: Image (inverted efficiency map, shared by all frames); ``x0``: [F,nx,ny,nz]
+    CUDA tensor (or one [nx,ny,nz] image replicated); center/size from ``effinv``."""
+
+    def __init__(self, model, frames, effinv, x0, n_subsets=1, use_graph=False):
+        if not isinstance(model, SplitLoRsModel):
+            raise TypeError("BatchedOSEM runs the TOR model (SplitLoRsModel)")
+        self.model = model
+        self.batch = FrameBatch(frames, n_subsets)
+        self.F = self.batch.n_frames
+        self.S = self.batch.n_subsets
+        grid = list(effinv.data.shape)
+        self.center, self.size = effinv.center, effinv.size
+        if x0.dim() == 3:
+            x0 = x0.unsqueeze(0).expand(self.F, *grid)
+        self.x = x0.contiguous().clone()
+        self.effinv = (effinv.data * float(self.S)).unsqueeze(0).expand(
+            self.F, *grid).contiguous()
+        probe = Image(torch.empty(grid, device=self.x.device), self.center, self.size)
+        self.geom = {a: model.kernel_geometry(probe, a)[1:] for a in model.AXIS}
+        self.use_graph = use_graph
+        self._graph = None
+        self.iteration = 0
+
+    def _subset_update(self, k):
+        m = self.model
+        bp = None
+        for a in m.AXIS:
+            lors, frame = self.batch.subsets[k][a]
+            g, c, s = self.geom[a]
+            if lors.shape[0] == 0:
+                continue
+            img_a = self.x.permute(*_stacked_perm(m.perm(a))).contiguous()
+            pv = ops.tor_projection_batched(lors, frame, img_a, self.F, g, c, s, m.kernel_width,
+                                            m.geo_sigma2_flag, m.tof_bin, m.tof_sigma2,
+                                            layout="nc")
+            bk = ops.tor_backprojection_batched(lors, frame, pv, self.F, g, c, s,
+                                                m.kernel_width, m.geo_sigma2_flag, m.tof_bin,
+                                                m.tof_sigma2, layout="nc")
+            back = bk.permute(*_stacked_perm(m.perm_back(a)))
+            bp = back.clone() if bp is None else bp.add_(back)
+        if bp is None:
+            bp = torch.zeros_like(self.x)
+        ops.mlem_update_(self.x, self.effinv, bp.contiguous())
+
+    def _iterate(self):
+        for k in range(self.S):
+            self._subset_update(k)
+
+    def _capture(self):
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        backup = self.x.clone()
+        with torch.cuda.stream(s):
+            self._iterate()
+        torch.cuda.current_stream().wait_stream(s)
+        self.x.copy_(backup)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._iterate()
+        self.x.copy_(backup)
+        self._graph = g
+
+    def step(self):
+        if self.use_graph:
+            if self._graph is None:
+                self._capture()
+            self._graph.replay()
+        else:
+            self._iterate()
+        self.iteration += 1
+        return self.x
+
+    def run(self, n_iterations):
+        for _ in range(n_iterations):
+            self.step()
+        return self.x

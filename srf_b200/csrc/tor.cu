@@ -32,6 +32,13 @@ namespace {
 
 enum TorOp { kProj = 0, kBack = 1, kMap = 2, kAdj = 3, kCount = 4 };
 
+// Process-wide tuning (srf_tor_set_tuning): kernel family (0 auto, 1 slab, 2 LOR-centric),
+// slices per slab (0 = as many as fit), grid multiplier of the persistent slab kernel
+// (CTAs = SMs x mult, one resident per SM: more, smaller shares of the segment list).
+std::atomic<int> g_tune_path{0};
+std::atomic<int> g_tune_nsl{0};
+std::atomic<int> g_tune_mult{1};
+
 struct TorParams {
     const float *x1, *y1, *z1, *x2, *y2, *z2, *xc, *yc, *zc, *f;
     int64_t stride, n;
@@ -51,7 +58,16 @@ struct TorParams {
     float *proj_out;
     int *count_out;   // kCount: [n] voxels with non-zero weight, [n] window voxels visited
     int use_slab;     // scatter ops: shared-memory slab kernel (1) or global atomics (0)
+    // Batched frames: LOR i belongs to frame frame[i] (null: one frame) whose image starts
+    // frame_stride floats after the previous frame's.
+    const int *frame;
+    int64_t frame_stride;
+    int n_frames;
 };
+
+__device__ __forceinline__ int64_t frame_offset(const TorParams &p, int64_t t) {
+    return p.frame ? (int64_t)__ldg(p.frame + t) * p.frame_stride : 0;
+}
 
 // slice_z of the reference launchers: float for projection (tor.cu.cc:380), a double
 // intermediate for back-projection and map (:423, :471).
@@ -76,6 +92,7 @@ __device__ __forceinline__ float fast_exp2(float x) {
 template <int OP>
 __device__ __noinline__ void generic_lor(const TorParams &p, int64_t t, int lane) {
     const int64_t slice_mesh = (int64_t)p.gx * p.gy;
+    const int64_t img0 = frame_offset(p, t);
     const int64_t o = t * p.stride;
     const float x1 = __ldg(p.x1 + o), y1 = __ldg(p.y1 + o), z1 = __ldg(p.z1 + o);
     const float x2 = __ldg(p.x2 + o), y2 = __ldg(p.y2 + o), z2 = __ldg(p.z2 + o);
@@ -163,12 +180,12 @@ __device__ __noinline__ void generic_lor(const TorParams &p, int64_t t, int lane
                         if (OP == kCount) {
                             n_useful++;
                         } else if (OP == kProj) {
-                            acc = fmaf(w, __ldg(p.image_in + row + ix), acc);
+                            acc = fmaf(w, __ldg(p.image_in + img0 + row + ix), acc);
                         } else {
-                            atomicAdd(p.image_out + row + ix, w * scale);
+                            atomicAdd(p.image_out + img0 + row + ix, w * scale);
                         }
                     } else if (OP == kMap && all_slots) {
-                        atomicAdd(p.image_out + row + ix, 0.0f * scale);
+                        atomicAdd(p.image_out + img0 + row + ix, 0.0f * scale);
                     }
                 }
             }
@@ -366,8 +383,9 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
         float acc = 0.0f;
         int n_useful = 0, n_slots = 0;
         if (any) {
+            const int64_t img0 = frame_offset(p, t);
             for (int s = L.s_lo + lane; s <= L.s_hi; s += 32) {
-                const int64_t base = (int64_t)s * slice_mesh;
+                const int64_t base = img0 + (int64_t)s * slice_mesh;
                 n_slots += slice_visit<OP, P>(p, L, s, [&](int idx, int, float w) {
                     if (OP == kCount) {
                         n_useful++;
@@ -422,7 +440,8 @@ constexpr int kSlabThreads = 1024;
 constexpr size_t kSlabSmemBytes = 220 * 1024;  // of the 227 KB a CTA can opt into
 
 struct SegPlan {
-    int nsl, n_slabs, ntiles;
+    int nsl, n_slabs, ntiles;  // n_slabs counts slab ids over all frames
+    int slabs_pf;              // slabs per frame
     int *range;            // [n] packed k_lo | k_hi << 16, or -1
     int *tile_counts;      // [ntiles * n_slabs]
     int64_t *tile_offs;    // [ntiles * n_slabs]
@@ -443,7 +462,8 @@ __global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams 
         bool ok = lor_slices(p, t, s_lo, s_hi);
         if (ok && OP == kBack) ok = (double)__ldg(p.values + t) > 1e-7;  // tor.cu.cc:203
         if (ok) {
-            const int k_lo = s_lo / sp.nsl, k_hi = s_hi / sp.nsl;
+            const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
+            const int k_lo = f0 + s_lo / sp.nsl, k_hi = f0 + s_hi / sp.nsl;
             packed = k_lo | (k_hi << 16);
             for (int k = k_lo; k <= k_hi; k++) atomicAdd(&hist[k], 1);
         }
@@ -566,7 +586,7 @@ __host__ __device__ __forceinline__ int slab_slice_stride(int gx, int gy) {
 }
 
 template <int OP, int P>
-__global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams p, SegPlan sp) {
+__global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorParams p, SegPlan sp) {
     extern __shared__ float slab[];
     __shared__ signed char owner_tab[kSlabThreads / 32][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -590,11 +610,13 @@ __global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams 
     while (pos < hi) {
         while (sp.slab_offs[k + 1] <= pos) k++;  // skip empty slabs
         const int64_t end = min(hi, sp.slab_offs[k + 1]);
-        const int S0 = k * sp.nsl;
+        const int fr = k / sp.slabs_pf;
+        const int S0 = (k - fr * sp.slabs_pf) * sp.nsl;
+        const int64_t img0 = (int64_t)fr * p.frame_stride;
         const int S1 = min(S0 + sp.nsl, p.gz);
         const int n_rows = (S1 - S0) * p.gy;
         if (OP == kProj) {
-            const float *src = p.image_in + (int64_t)S0 * slice_mesh;
+            const float *src = p.image_in + img0 + (int64_t)S0 * slice_mesh;
             for (int r = warp; r < n_rows; r += kWarps) {
                 const int sl = r / p.gy, iy = r - sl * p.gy;
                 const float *g = src + (int64_t)r * p.gx;
@@ -669,7 +691,7 @@ __global__ void __launch_bounds__(kSlabThreads) tor_slab_kernel(const TorParams 
         }
         __syncthreads();
         if (OP != kProj) {
-            float *out = p.image_out + (int64_t)S0 * slice_mesh;
+            float *out = p.image_out + img0 + (int64_t)S0 * slice_mesh;
             for (int r = warp; r < n_rows; r += kWarps) {
                 const int sl = r / p.gy, iy = r - sl * p.gy;
                 const float *src = slab + sl * ss + iy * rs;
@@ -730,11 +752,9 @@ int tor_setup(TorParams &p, const int *grid, const float *center, const float *s
                            : 1.0f;
     p.n = n;
     p.stride = lor_stride;
-    // Kernel selection: the shared-memory slab kernels by default (when a slice fits in
-    // shared memory); SRF_TOR_SCATTER=global selects the LOR-centric kernels (gathers from
-    // L2, global atomics), the fallback for larger slices, so that tests exercise both.
-    const char *env = std::getenv("SRF_TOR_SCATTER");
-    p.use_slab = (env && env[0] == 'g') ? 0 : 1;
+    // Kernel family: the shared-memory slab kernels unless tuning selects the LOR-centric
+    // ones (gathers from L2, global atomics; also the fallback when a slice does not fit).
+    p.use_slab = g_tune_path.load(std::memory_order_relaxed) == 2 ? 0 : 1;
     return SRF_OK;
 }
 
@@ -748,20 +768,24 @@ void launch_p(const TorParams &p, int grid, int block, cudaStream_t stream) {
 bool slab_geometry(const TorParams &p, int &nsl, int &n_slabs) {
     if (p.gx > (1 << 15) || p.gy > (1 << 15)) return false;
     const size_t slice_bytes = sizeof(float) * (size_t)slab_slice_stride(p.gx, p.gy);
-    if (slice_bytes > kSlabSmemBytes) return false;
-    nsl = (int)std::min<size_t>(kSlabSmemBytes / slice_bytes, (size_t)p.gz);
+    const size_t budget = kSlabSmemBytes;
+    if (slice_bytes > budget) return false;
+    nsl = (int)std::min<size_t>(budget / slice_bytes, (size_t)p.gz);
+    const int want = g_tune_nsl.load(std::memory_order_relaxed);
+    if (want > 0) nsl = std::min(nsl, want);
     n_slabs = (p.gz + nsl - 1) / nsl;
-    return n_slabs <= kMaxSlabs && p.n < (int64_t)INT32_MAX;
+    return (int64_t)n_slabs * std::max(1, p.n_frames) <= kMaxSlabs && p.n < (int64_t)INT32_MAX;
 }
 
 template <int OP, int P>
 int launch_slab(const TorParams &p, cudaStream_t stream) {
     SegPlan sp{};
-    if (!slab_geometry(p, sp.nsl, sp.n_slabs)) return -1;
+    if (!slab_geometry(p, sp.nsl, sp.slabs_pf)) return -1;
+    sp.n_slabs = sp.slabs_pf * std::max(1, p.n_frames);
     sp.ntiles = (int)((p.n + kSegTile - 1) / kSegTile);
     // Scratch from the stream-ordered pool: no host synchronisation, capturable. The
     // segment list is sized for the worst case (every LOR in every slab it can reach).
-    const int64_t max_slabs_per_lor = sp.n_slabs;
+    const int64_t max_slabs_per_lor = sp.slabs_pf;
     const size_t cap = (size_t)p.n * (size_t)max_slabs_per_lor;
     auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
     const size_t b_range = al(sizeof(int) * p.n);
@@ -810,7 +834,8 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
     seg_scan_kernel<<<sp.n_slabs, 1024, 0, stream>>>(sp, slab_tot);
     seg_offsets_kernel<<<1, 32, 0, stream>>>(sp, slab_tot);
     seg_fill_kernel<<<sp.ntiles, kSegThreads, 0, stream>>>(p, sp);
-    tor_slab_kernel<OP, P><<<num_sms(), kSlabThreads, smem, stream>>>(p, sp);
+    const int mult = std::max(1, std::min(8, g_tune_mult.load(std::memory_order_relaxed)));
+    tor_slab_kernel<OP, P><<<num_sms() * mult, kSlabThreads, smem, stream>>>(p, sp);
     int st = check_launch();
     e = cudaFreeAsync(ws, stream);
     if (st == SRF_OK && e != cudaSuccess) {
@@ -991,4 +1016,125 @@ extern "C" int srf_tor_backproject_adjoint(const float *x1, const float *y1, con
     p.values = values;
     p.image_out = image;
     return tor_launch<kAdj>(p, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------------------------ batched frames
+// No counterpart in the reference: many independent reconstructions sharing one
+// geometry in one launch. LOR i belongs to frame frame[i] in [0, n_frames); the images
+// are n_frames consecutive blocks of frame_stride floats (frame_stride >= voxels).
+
+namespace {
+int set_frames(TorParams &p, const int *frame, int n_frames, int64_t frame_stride) {
+    const int64_t nvox = (int64_t)p.gx * p.gy * p.gz;
+    if (n_frames < 1 || (p.n > 0 && !frame) || frame_stride < nvox) return SRF_ERR_INVALID_ARGUMENT;
+    if ((int64_t)n_frames * frame_stride > ((int64_t)1 << 40)) return SRF_ERR_UNSUPPORTED;
+    p.frame = frame;
+    p.n_frames = n_frames;
+    p.frame_stride = frame_stride;
+    return SRF_OK;
+}
+
+int zero_frames(float *image, int n_frames, int64_t frame_stride, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(image, 0, sizeof(float) * (size_t)n_frames * frame_stride,
+                                    stream);
+    if (e != cudaSuccess) {
+        set_cuda_error(e);
+        return SRF_ERR_CUDA;
+    }
+    return SRF_OK;
+}
+}  // namespace
+
+extern "C" int srf_tor_projection_batched(
+    const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
+    const float *z2, const float *xc, const float *yc, const float *zc,
+    const float *sigma2_factor, int geo_sigma2_flag, const int *frame, int n_frames,
+    int64_t frame_stride, float *projection_value, const int *grid, const float *center,
+    const float *size, float kernel_width, float tof_bin, float tof_sigma2, const float *images,
+    int64_t num_events, int64_t lor_stride, void *stream) {
+    TorParams p{};
+    int st = tor_setup(p, grid, center, size, kernel_width, tof_bin, tof_sigma2, num_events,
+                       lor_stride);
+    if (st != SRF_OK) return st;
+    if ((st = set_frames(p, frame, n_frames, frame_stride)) != SRF_OK) return st;
+    if (num_events > 0 &&
+        !cols_ok({x1, y1, z1, x2, y2, z2, sigma2_factor, projection_value, images}))
+        return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > 0 && p.tof_on && !cols_ok({xc, yc, zc})) return SRF_ERR_INVALID_ARGUMENT;
+    p.x1 = x1; p.y1 = y1; p.z1 = z1; p.x2 = x2; p.y2 = y2; p.z2 = z2;
+    p.xc = xc; p.yc = yc; p.zc = zc; p.f = sigma2_factor;
+    p.geo = geo_sigma2_flag != 0;
+    p.image_in = images;
+    p.proj_out = projection_value;
+    return tor_launch<kProj>(p, (cudaStream_t)stream);
+}
+
+namespace {
+template <int OP>
+int scatter_batched(const float *x1, const float *y1, const float *z1, const float *x2,
+                    const float *y2, const float *z2, const float *xc, const float *yc,
+                    const float *zc, const float *sigma2_factor, int geo_sigma2_flag,
+                    const int *frame, int n_frames, int64_t frame_stride, const float *values,
+                    const int *grid, const float *center, const float *size, float kernel_width,
+                    float tof_bin, float tof_sigma2, float *images, int64_t num_events,
+                    int64_t lor_stride, int accumulate, void *stream) {
+    TorParams p{};
+    int st = tor_setup(p, grid, center, size, kernel_width, tof_bin, tof_sigma2, num_events,
+                       lor_stride);
+    if (st != SRF_OK) return st;
+    if ((st = set_frames(p, frame, n_frames, frame_stride)) != SRF_OK) return st;
+    if (!images) return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > 0 && !cols_ok({x1, y1, z1, x2, y2, z2, sigma2_factor, values}))
+        return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > 0 && p.tof_on && !cols_ok({xc, yc, zc})) return SRF_ERR_INVALID_ARGUMENT;
+    if (!accumulate &&
+        (st = zero_frames(images, n_frames, frame_stride, (cudaStream_t)stream)) != SRF_OK)
+        return st;
+    p.x1 = x1; p.y1 = y1; p.z1 = z1; p.x2 = x2; p.y2 = y2; p.z2 = z2;
+    p.xc = xc; p.yc = yc; p.zc = zc; p.f = sigma2_factor;
+    p.geo = geo_sigma2_flag != 0;
+    p.values = values;
+    p.image_out = images;
+    return tor_launch<OP>(p, (cudaStream_t)stream);
+}
+}  // namespace
+
+extern "C" int srf_tor_backprojection_batched(
+    const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
+    const float *z2, const float *xc, const float *yc, const float *zc,
+    const float *sigma2_factor, int geo_sigma2_flag, const int *frame, int n_frames,
+    int64_t frame_stride, const float *projection_value, const int *grid, const float *center,
+    const float *size, float kernel_width, float tof_bin, float tof_sigma2, float *images,
+    int64_t num_events, int64_t lor_stride, int accumulate, void *stream) {
+    return scatter_batched<kBack>(x1, y1, z1, x2, y2, z2, xc, yc, zc, sigma2_factor,
+                                  geo_sigma2_flag, frame, n_frames, frame_stride,
+                                  projection_value, grid, center, size, kernel_width, tof_bin,
+                                  tof_sigma2, images, num_events, lor_stride, accumulate,
+                                  stream);
+}
+
+extern "C" int srf_tor_backproject_adjoint_batched(
+    const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
+    const float *z2, const float *xc, const float *yc, const float *zc,
+    const float *sigma2_factor, int geo_sigma2_flag, const int *frame, int n_frames,
+    int64_t frame_stride, const float *values, const int *grid, const float *center,
+    const float *size, float kernel_width, float tof_bin, float tof_sigma2, float *images,
+    int64_t num_events, int64_t lor_stride, int accumulate, void *stream) {
+    return scatter_batched<kAdj>(x1, y1, z1, x2, y2, z2, xc, yc, zc, sigma2_factor,
+                                 geo_sigma2_flag, frame, n_frames, frame_stride, values, grid,
+                                 center, size, kernel_width, tof_bin, tof_sigma2, images,
+                                 num_events, lor_stride, accumulate, stream);
+}
+
+// No counterpart in the reference: process-wide kernel tuning for the TOR ops, used by
+// the autotuner. path: 0 automatic (slab kernels when a slice fits in shared memory),
+// 1 slab kernels, 2 LOR-centric kernels; slab_slices: slices per shared-memory slab
+// (0 = as many as fit); grid_mult: persistent slab CTAs = SMs x grid_mult (1..8).
+extern "C" int srf_tor_set_tuning(int path, int slab_slices, int grid_mult) {
+    if (path < 0 || path > 2 || slab_slices < 0 || grid_mult < 1 || grid_mult > 8)
+        return SRF_ERR_INVALID_ARGUMENT;
+    g_tune_path.store(path);
+    g_tune_nsl.store(slab_slices);
+    g_tune_mult.store(grid_mult);
+    return SRF_OK;
 }

@@ -284,3 +284,74 @@ def mlem_update_(image, effinv, bp):
         _call(dev, "srf_mlem_update", image.data_ptr(), effinv.data_ptr(), bp.data_ptr(),
                   image.numel(), _stream(dev))
     return image
+
+
+# ------------------------------------------------------------------ batched frames
+
+
+def _frame_args(frame, n_frames, images_numel, g):
+    if frame is None or frame.dtype != torch.int32 or not frame.is_cuda:
+        raise TypeError("frame must be a CUDA int32 tensor")
+    nvox = g[0] * g[1] * g[2]
+    if images_numel != n_frames * nvox:
+        raise ValueError(f"images hold {images_numel} voxels, {n_frames} frames need "
+                         f"{n_frames * nvox}")
+    return frame.contiguous(), nvox
+
+
+def tor_projection_batched(lors, frame, images, n_frames, grid, center, size, kernel_width,
+                           geo_sigma2_flag=False, tof_bin=1.0e4, tof_sigma2=1.0e4,
+                           layout="auto", out=None):
+    """Projection of LOR i through image images[frame[i]]; images [F, g2, g1, g0]."""
+    dev = _check_cuda(lors, images, out)
+    t, cols, n, stride = _columns(lors, TOR_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    fr, nvox = _frame_args(frame, n_frames, images.numel(), g)
+    if fr.numel() != n:
+        raise ValueError("frame needs one entry per LOR")
+    imgs = images.contiguous()
+    if out is None:
+        out = torch.empty(n, dtype=torch.float32, device=dev)
+    with torch.cuda.device(dev):
+        _call(dev, "srf_tor_projection_batched", *cols[:10], int(bool(geo_sigma2_flag)),
+              fr.data_ptr(), int(n_frames), nvox, out.data_ptr(), ga, ca, sa,
+              float(kernel_width), float(tof_bin), float(tof_sigma2), imgs.data_ptr(), n, stride,
+              _stream(dev))
+    return out
+
+
+def _tor_scatter_batched(fn, lors, frame, values, n_frames, grid, center, size, kernel_width,
+                         geo_sigma2_flag, tof_bin, tof_sigma2, layout, out, accumulate):
+    dev = _check_cuda(lors, values, out)
+    t, cols, n, stride = _columns(lors, TOR_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    nvox = g[0] * g[1] * g[2]
+    if out is None:
+        out = torch.empty((n_frames, g[2], g[1], g[0]), dtype=torch.float32, device=dev)
+        accumulate = False
+    fr, _ = _frame_args(frame, n_frames, out.numel(), g)
+    v = _values(values, n)
+    with torch.cuda.device(dev):
+        _call(dev, fn, *cols[:10], int(bool(geo_sigma2_flag)), fr.data_ptr(), int(n_frames), nvox,
+              v.data_ptr(), ga, ca, sa, float(kernel_width), float(tof_bin), float(tof_sigma2),
+              out.data_ptr(), n, stride, int(bool(accumulate)), _stream(dev))
+    return out
+
+
+def tor_backprojection_batched(lors, frame, lors_value, n_frames, grid, center, size,
+                               kernel_width, geo_sigma2_flag=False, tof_bin=1.0e4,
+                               tof_sigma2=1.0e4, layout="auto", out=None, accumulate=False):
+    """Reference back-projection A^T(1/v) of each LOR into its frame's image."""
+    return _tor_scatter_batched("srf_tor_backprojection_batched", lors, frame, lors_value,
+                                n_frames, grid, center, size, kernel_width, geo_sigma2_flag,
+                                tof_bin, tof_sigma2, layout, out, accumulate)
+
+
+def tor_backproject_adjoint_batched(values, lors, frame, n_frames, grid, center, size,
+                                    kernel_width, geo_sigma2_flag=False, tof_bin=1.0e4,
+                                    tof_sigma2=1.0e4, layout="auto", out=None,
+                                    accumulate=False):
+    """Plain adjoint A^T values per frame."""
+    return _tor_scatter_batched("srf_tor_backproject_adjoint_batched", lors, frame, values,
+                                n_frames, grid, center, size, kernel_width, geo_sigma2_flag,
+                                tof_bin, tof_sigma2, layout, out, accumulate)

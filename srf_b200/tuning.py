@@ -1,0 +1,78 @@
+"""Kernel tuning for the TOR ops and a small autotuner.
+
+``set_tuning(path, slab_slices, grid_mult)`` sets the library's process-wide knobs
+(``srf_tor_set_tuning``): the kernel family (0 automatic, 1 shared-memory slabs,
+2 LOR-centric), the number of slices per shared-memory slab (0 = as many as fit) and
+the grid multiplier of the persistent slab kernel.
+
+``Autotuner`` times a caller-supplied step (for example one OSEM sub-iteration on a
+representative subset) under each candidate setting with CUDA events and keeps the
+fastest per key (geometry, patch size, problem size bucket); results can be saved to and
+loaded from a JSON file so a reconstruction tunes once per configuration.
+"""
+
+import json
+import math
+import os
+
+import torch
+
+from . import _lib
+
+DEFAULT = (0, 0, 1)
+
+
+def set_tuning(path=0, slab_slices=0, grid_mult=1):
+    _lib.call("srf_tor_set_tuning", int(path), int(slab_slices), int(grid_mult))
+    return (path, slab_slices, grid_mult)
+
+
+def candidates(max_slab_slices):
+    """Settings worth trying: full and half-depth slabs, grid multipliers 1 and 2, and
+    the LOR-centric kernels."""
+    out = [(1, 0, 1), (1, 0, 2)]
+    half = max(1, max_slab_slices // 2)
+    if half < max_slab_slices:
+        out += [(1, half, 1), (1, half, 2)]
+    out.append((2, 0, 1))
+    return out
+
+
+def key_for(grid, patch, n_lors, n_frames=1):
+    bucket = int(math.log2(max(1, n_lors)))
+    return f"g{grid[0]}x{grid[1]}x{grid[2]}_p{patch}_n2^{bucket}_f{n_frames}"
+
+
+class Autotuner:
+    def __init__(self, cache_path=None):
+        self.cache_path = cache_path
+        self.table = {}
+        if cache_path and os.path.exists(cache_path):
+            with open(cache_path) as f:
+                self.table = {k: tuple(v) for k, v in json.load(f).items()}
+
+    def tune(self, key, step, cands, warmup=1, reps=3):
+        """Time ``step()`` under each setting of ``cands``; apply and return the best."""
+        if key in self.table:
+            set_tuning(*self.table[key])
+            return self.table[key], None
+        timings = {}
+        for c in cands:
+            set_tuning(*c)
+            for _ in range(warmup):
+                step()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            s.record()
+            for _ in range(reps):
+                step()
+            e.record()
+            torch.cuda.synchronize()
+            timings[c] = s.elapsed_time(e) / reps
+        best = min(timings, key=timings.get)
+        self.table[key] = best
+        set_tuning(*best)
+        if self.cache_path:
+            with open(self.cache_path, "w") as f:
+                json.dump({k: list(v) for k, v in self.table.items()}, f, indent=1)
+        return best, timings

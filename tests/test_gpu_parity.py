@@ -70,13 +70,15 @@ def tcase():
 
 
 @pytest.fixture(params=["slab", "global"])
-def tor_path(request, monkeypatch):
+def tor_path(request):
     """The TOR ops have two kernel families: shared-memory slabs (default) and
     LOR-centric kernels reading the image from L2 with global atomics
-    (SRF_TOR_SCATTER=global, the fallback when a slice does not fit in shared memory).
+    (tuning path 2, the fallback when a slice does not fit in shared memory).
     Both must agree with the oracle."""
-    monkeypatch.setenv("SRF_TOR_SCATTER", request.param)
-    return request.param
+    from srf_b200 import tuning
+    tuning.set_tuning(path=1 if request.param == "slab" else 2)
+    yield request.param
+    tuning.set_tuning()
 
 
 @pytest.mark.parametrize("pname", list(TOR_PARAMS))
@@ -100,12 +102,14 @@ def test_tor_projection(tcase, pname, axis, tor_path):
 
 
 @pytest.fixture(params=["slab", "global"])
-def scatter_kernel(request, monkeypatch):
+def scatter_kernel(request):
     """Back-projection / map / adjoint have two kernels: shared-memory slabs (default)
-    and global atomics (SRF_TOR_SCATTER=global, the fallback when a slice does not fit
-    in shared memory). Both must agree with the oracle."""
-    monkeypatch.setenv("SRF_TOR_SCATTER", request.param)
-    return request.param
+    and global atomics (tuning path 2, the fallback when a slice does not fit in shared
+    memory). Both must agree with the oracle."""
+    from srf_b200 import tuning
+    tuning.set_tuning(path=1 if request.param == "slab" else 2)
+    yield request.param
+    tuning.set_tuning()
 
 
 @pytest.mark.parametrize("pname", ["tof530_kw10", "tof530_kw4_geo", "notof"])

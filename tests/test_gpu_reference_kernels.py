@@ -32,9 +32,11 @@ def tcase():
 
 
 @pytest.fixture(params=["slab", "global"])
-def tor_path(request, monkeypatch):
-    monkeypatch.setenv("SRF_TOR_SCATTER", request.param)
-    return request.param
+def tor_path(request):
+    from srf_b200 import tuning
+    tuning.set_tuning(path=1 if request.param == "slab" else 2)
+    yield request.param
+    tuning.set_tuning()
 
 
 @pytest.mark.parametrize("kw,geo", [(K.KW_CONFIG, False), (4.0, True)])
