@@ -336,15 +336,17 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
         const int j_lo = max(0, -iy0), j_hi = min(P, p.gy - iy0);
         n_slots = max(0, i_hi - i_lo) * max(0, j_hi - j_lo);
     }
+    // Column terms once per slice. Only the slice bounds gate a column: in the unrolled
+    // slot loop a column outside the tube costs the same issue slots either way and
+    // fails the exact cut-off test by itself.
     float dxs[P];
     unsigned colmask = 0u;
+    const float fx0 = (float)ix0;
 #pragma unroll
     for (int i = 0; i < P; i++) {
-        const int ix = ix0 + i;
-        const float mx = __fmaf_rn(p.inter_x, (float)ix + 0.5f, p.l_bound);
+        const float mx = __fmaf_rn(p.inter_x, fx0 + ((float)i + 0.5f), p.l_bound);
         dxs[i] = __fsub_rn(cx, mx);
-        const bool ok = (unsigned)ix < (unsigned)p.gx && dxs[i] * dxs[i] * L.q_col <= L.cut_skip;
-        colmask |= ok ? (1u << i) : 0u;
+        colmask |= ((unsigned)(ix0 + i) < (unsigned)p.gx) ? (1u << i) : 0u;
     }
     if (colmask == 0u) return n_slots;
 #pragma unroll
