@@ -24,6 +24,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdlib>
+#include <type_traits>
 
 #include "srf_common.cuh"
 
@@ -52,6 +53,8 @@ struct TorParams {
     float tse;        // tof_sigma2 + tof_bin^2/12, float as in tor.cu.cc:88
     float a_coef;     // log2(e) / (2 tse)
     float tof_scale;  // tof_bin / sqrt(2 pi tof_sigma2), or 1 without TOF
+    float inv_x, inv_y;  // 1/inter_x, 1/inter_y (window bounding boxes only)
+    float box_e;         // d^2 margin of the bounding boxes, far above float d^2 error
     const float *image_in;
     const float *values;
     float *image_out;
@@ -221,18 +224,20 @@ __global__ void __launch_bounds__(256) tor_kernel(const TorParams p) {
 //
 // Same traversal and the same float arithmetic for every quantity the reference
 // rounds, with three changes that cut the instruction count per voxel slot:
+//  * only the part of the P x P window inside the bounding box of the tube's section
+//    is walked. With d^2 = dx^2 + dy^2 - (dx ux + dy uy)^2 and q = 1 - ux^2 - uy^2, the
+//    set d^2 < c is an ellipse whose half-extents are sqrt(c (1 - uy^2) / q) along x and
+//    sqrt(c (1 - ux^2) / q) along y. The box is taken for c = cut + box_e, box_e far
+//    above the float error of d^2, so it holds every voxel the reference weights non-zero;
+//    each voxel in it still takes the exact float test. For dominant-axis LOR groups
+//    q >= 1/3 and the box is 4-5 voxels wide where the window is 6;
 //  * the P column offsets dx_i = X_x - mesh_x(i) are computed once per slice;
-//  * rows and columns that cannot hold a voxel inside the cut-off are skipped: over
-//    a row at offset dy the smallest d^2 is dy^2 uz^2/(1 - ux^2) (minimising the
-//    quadratic in dx), over a column dx^2 uz^2/(1 - uy^2); a row/column is skipped
-//    only when that bound exceeds the cut-off with a 0.1 % margin, far above the float
-//    error of d^2, so every voxel the reference weights non-zero is still evaluated
-//    with the exact test;
 //  * the weight is one raw ex2 and the slot test is predicated, not branched.
 
 struct LorConst {
     float x1, y1, z1, d0, d1, dz, ux, uy;
-    float cut, k1, q_row, q_col, cut_skip;
+    float cut, k1;
+    float bxv, byv;  // bounding-box half-extents in voxels (margin included)
     float xc, yc, zc;
     float scale;
     int s_lo, s_hi;  // candidate slices (a superset; each is tested exactly)
@@ -277,12 +282,15 @@ __device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorCo
         const float inv = 0.5f * kLog2e / tsc;
         L.k1 = (p.tof_on && OP != kMap) ? (p.a_coef - inv) : -inv;
     }
-    const float uz = L.dz / dis;
-    const float om_x = 1.0f - L.ux * L.ux, om_y = 1.0f - L.uy * L.uy;
-    const bool prune = om_x > 0.01f && om_y > 0.01f && !L.all;
-    L.q_row = prune ? uz * uz / om_x : 0.0f;
-    L.q_col = prune ? uz * uz / om_y : 0.0f;
-    L.cut_skip = L.cut * 1.001f + 1e-6f;
+    {
+        const float om_x = 1.0f - L.ux * L.ux, om_y = 1.0f - L.uy * L.uy;
+        const float q = om_x - L.uy * L.uy;
+        const float c = L.cut * 1.0001f + p.box_e;
+        const bool boxed = q > 1e-3f && !L.all && c < 3.0e38f;
+        // outside a box (nearly in-plane LOR, map LOR with a zero divisor): whole window
+        L.bxv = boxed ? sqrtf(c * om_y / q) * p.inv_x + (1.0f / 1024.0f) : 1.0e9f;
+        L.byv = boxed ? sqrtf(c * om_x / q) * p.inv_y + (1.0f / 1024.0f) : 1.0e9f;
+    }
     L.xc = L.yc = L.zc = 0.0f;
     if (OP != kMap && OP != kCount && p.tof_on) {
         L.xc = __ldg(p.xc + o);
@@ -310,62 +318,130 @@ __device__ __forceinline__ bool lor_slices(const TorParams &p, int64_t t, int &s
     return s_lo <= s_hi;
 }
 
+// One voxel slot: the reference's d^2 (tor.cu.cc:61-66, FMA-contracted as nvcc builds
+// it) and cut-off decision, and the folded exponent.
+template <int OP, typename F>
+__device__ __forceinline__ void slot(const LorConst &L, float dx, float dyuy, float dy2, float k0,
+                                     int ix, int iy, F &f) {
+    const float rc = __fmaf_rn(dx, L.ux, dyuy);
+    const float d2 = __fmaf_rn(-rc, rc, __fmaf_rn(dx, dx, dy2));
+    const bool in_cut = d2 < L.cut;
+    const float e = fast_exp2(fmaf(d2, L.k1, k0));
+    if (OP == kMap)
+        f(ix, iy, in_cut ? e : 0.0f, in_cut || L.all);
+    else
+        f(ix, iy, e, in_cut);
+}
+
+// W consecutive slots of one row.
+template <int OP, int W, int P, typename F>
+__device__ __forceinline__ void row_slots(const LorConst &L, const float (&dxs)[P], float dy,
+                                          float k0, int xlo, int iy, F &f) {
+    const float dyuy = __fmul_rn(dy, L.uy);
+    const float dy2 = __fmul_rn(dy, dy);
+#pragma unroll
+    for (int i = 0; i < W; i++) slot<OP>(L, dxs[i], dyuy, dy2, k0, xlo + i, iy, f);
+}
+
+// g(std::integral_constant<int, w>{}) for a runtime width 1 <= w <= P.
+template <int P, typename G>
+__device__ __forceinline__ void with_width(int w, G &&g) {
+    if constexpr (P >= 1) {
+        if (w >= P) {
+            g(std::integral_constant<int, P>{});
+        } else {
+            with_width<P - 1>(w, g);
+        }
+    }
+}
+
 // One (LOR, slice): the reference's crossing test and window (tor.cu.cc:22-48,
-// :135-136), then every voxel with non-zero weight: f(index_in_slice, row, w) with w the
-// unscaled weight (for a map LOR with L.all set, every in-slice window voxel, with
+// :135-136), then the voxels of the window's part inside the tube's bounding box:
+// f(ix, iy, w, use) with w the unscaled weight and use the reference's decision (d^2
+// below the cut-off; for a map LOR with L.all set, every in-slice window voxel, with
 // w = 0 outside the cut-off, as the reference adds 0/0 there). Returns the number of
 // in-slice window voxels (for kCount).
-template <int OP, int P, typename F>
+//
+// kPadded: the caller's slice has P - 1 zero rows and columns around the grid (the
+// shared-memory slab), so window voxels outside the grid need no test: a gather reads 0
+// there and a scatter lands in padding that is never flushed. The walked box is then
+// widened to the warp's largest (kept inside the window), which makes the trip counts
+// warp-uniform. Otherwise the box is clipped to the grid.
+template <int OP, int P, bool kPadded, typename F>
 __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L, int s, F &&f) {
     const float sz = slice_z<OP>(p, s);
     const float ratio = __fdiv_rn(__fsub_rn(sz, L.z1), L.dz);
     if (!(ratio > 0.0f && ratio < 1.0f)) return 0;
     const float cx = __fmaf_rn(L.d0, ratio, L.x1);
     const float cy = __fmaf_rn(L.d1, ratio, L.y1);
-    const int ix0 = __float2int_rz(__fdiv_rn(__fsub_rn(cx, p.l_bound), p.inter_x)) - p.half;
-    const int iy0 = __float2int_rz(__fdiv_rn(__fsub_rn(cy, p.b_bound), p.inter_y)) - p.half;
+    const float rx = __fsub_rn(cx, p.l_bound), ry = __fsub_rn(cy, p.b_bound);
+    const int ix0 = __float2int_rz(__fdiv_rn(rx, p.inter_x)) - p.half;
+    const int iy0 = __float2int_rz(__fdiv_rn(ry, p.inter_y)) - p.half;
+    if (ix0 >= p.gx || iy0 >= p.gy || ix0 <= -P || iy0 <= -P) return 0;  // window off the grid
+    int n_slots = 0;
+    if (OP == kCount) {
+        const int i_lo = max(0, -ix0), i_hi = min(P, p.gx - ix0);
+        const int j_lo = max(0, -iy0), j_hi = min(P, p.gy - iy0);
+        n_slots = (i_hi - i_lo) * (j_hi - j_lo);
+    }
+    // Bounding box in voxel-centre units (column i has its centre at i + 0.5 voxels).
+    const float fx = __fmaf_rn(rx, p.inv_x, -0.5f), fy = __fmaf_rn(ry, p.inv_y, -0.5f);
+    int xlo = max(ix0, __float2int_ru(fx - L.bxv));
+    int xhi = min(ix0 + P - 1, __float2int_rd(fx + L.bxv));
+    int ylo = max(iy0, __float2int_ru(fy - L.byv));
+    int yhi = min(iy0 + P - 1, __float2int_rd(fy + L.byv));
+    if (!kPadded) {
+        xlo = max(xlo, 0);
+        xhi = min(xhi, p.gx - 1);
+        ylo = max(ylo, 0);
+        yhi = min(yhi, p.gy - 1);
+    }
+    int wx = xhi - xlo + 1, wy = yhi - ylo + 1;
+    if (wx <= 0 || wy <= 0) return n_slots;
+    if (kPadded) {
+        const unsigned am = __activemask();
+        const int mx = __reduce_max_sync(am, wx), my = __reduce_max_sync(am, wy);
+        xlo = min(xlo, ix0 + P - mx);  // still inside the window, still covers the box
+        ylo = min(ylo, iy0 + P - my);
+        wx = mx;
+        wy = my;
+    }
     float k0 = 0.0f;
     if (OP != kMap && OP != kCount && p.tof_on) {
         const float ax = __fsub_rn(L.xc, cx), ay = __fsub_rn(L.yc, cy), az = __fsub_rn(L.zc, sz);
         const float a2 = __fmaf_rn(az, az, __fmaf_rn(ax, ax, __fmul_rn(ay, ay)));
         k0 = -a2 * p.a_coef;
     }
-    int n_slots = 0;
-    if (OP == kCount) {
-        const int i_lo = max(0, -ix0), i_hi = min(P, p.gx - ix0);
-        const int j_lo = max(0, -iy0), j_hi = min(P, p.gy - iy0);
-        n_slots = max(0, i_hi - i_lo) * max(0, j_hi - j_lo);
-    }
-    // Column terms once per slice. Only the slice bounds gate a column: in the unrolled
-    // slot loop a column outside the tube costs the same issue slots either way and
-    // fails the exact cut-off test by itself.
     float dxs[P];
-    unsigned colmask = 0u;
-    const float fx0 = (float)ix0;
+    const float fx0 = (float)xlo;
 #pragma unroll
     for (int i = 0; i < P; i++) {
-        const float mx = __fmaf_rn(p.inter_x, fx0 + ((float)i + 0.5f), p.l_bound);
-        dxs[i] = __fsub_rn(cx, mx);
-        colmask |= ((unsigned)(ix0 + i) < (unsigned)p.gx) ? (1u << i) : 0u;
+        const float mxi = __fmaf_rn(p.inter_x, fx0 + ((float)i + 0.5f), p.l_bound);
+        dxs[i] = __fsub_rn(cx, mxi);
     }
-    if (colmask == 0u) return n_slots;
+    if (kPadded) {
+        // wx, wy are warp-uniform: one fully unrolled row body per width, so that the
+        // row's loads issue back to back.
+        for (int j = 0; j < wy; j++) {
+            const int iy = ylo + j;
+            const float dy = __fsub_rn(cy, __fmaf_rn(p.inter_y, (float)iy + 0.5f, p.b_bound));
+            with_width<P>(wx, [&](auto W) {
+                row_slots<OP, decltype(W)::value>(L, dxs, dy, k0, xlo, iy, f);
+            });
+        }
+    } else {
 #pragma unroll
-    for (int j = 0; j < P; j++) {
-        const int iy = iy0 + j;
-        const float my = __fmaf_rn(p.inter_y, (float)iy + 0.5f, p.b_bound);
-        const float dy = __fsub_rn(cy, my);
-        if ((unsigned)iy >= (unsigned)p.gy || dy * dy * L.q_row > L.cut_skip) continue;
-        const float dyuy = __fmul_rn(dy, L.uy);
-        const float dy2 = __fmul_rn(dy, dy);
-        const int row = iy * p.gx + ix0;
+        for (int j = 0; j < P; j++) {
+            if (j >= wy) break;
+            const int iy = ylo + j;
+            const float dy = __fsub_rn(cy, __fmaf_rn(p.inter_y, (float)iy + 0.5f, p.b_bound));
+            const float dyuy = __fmul_rn(dy, L.uy);
+            const float dy2 = __fmul_rn(dy, dy);
 #pragma unroll
-        for (int i = 0; i < P; i++) {
-            const float rc = __fmaf_rn(dxs[i], L.ux, dyuy);
-            const float d2 = __fmaf_rn(-rc, rc, __fmaf_rn(dxs[i], dxs[i], dy2));
-            const bool in_cut = d2 < L.cut;
-            const bool use = ((colmask >> i) & 1u) && (in_cut || L.all);
-            const float w = in_cut ? fast_exp2(fmaf(d2, L.k1, k0)) : 0.0f;
-            if (use) f(row + i, iy, w);
+            for (int i = 0; i < P; i++) {
+                if (i >= wx) break;
+                slot<OP>(L, dxs[i], dyuy, dy2, k0, xlo + i, iy, f);
+            }
         }
     }
     return n_slots;
@@ -388,13 +464,15 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
             const int64_t img0 = frame_offset(p, t);
             for (int s = L.s_lo + lane; s <= L.s_hi; s += 32) {
                 const int64_t base = img0 + (int64_t)s * slice_mesh;
-                n_slots += slice_visit<OP, P>(p, L, s, [&](int idx, int, float w) {
+                n_slots += slice_visit<OP, P, false>(p, L, s,
+                                                     [&](int ix, int iy, float w, bool use) {
+                    const int64_t idx = base + (int64_t)iy * p.gx + ix;
                     if (OP == kCount) {
-                        n_useful++;
+                        n_useful += use ? 1 : 0;
                     } else if (OP == kProj) {
-                        acc = fmaf(w, __ldg(p.image_in + base + idx), acc);
+                        if (use) acc = fmaf(w, __ldg(p.image_in + idx), acc);
                     } else {
-                        atomicAdd(p.image_out + base + idx, w * L.scale);
+                        if (use) atomicAdd(p.image_out + idx, w * L.scale);
                     }
                 });
             }
@@ -562,9 +640,8 @@ __device__ __forceinline__ LorConst shfl_lor(const LorConst &L, int src) {
     M.uy = __shfl_sync(0xffffffffu, L.uy, src);
     M.cut = __shfl_sync(0xffffffffu, L.cut, src);
     M.k1 = __shfl_sync(0xffffffffu, L.k1, src);
-    M.q_row = __shfl_sync(0xffffffffu, L.q_row, src);
-    M.q_col = __shfl_sync(0xffffffffu, L.q_col, src);
-    M.cut_skip = __shfl_sync(0xffffffffu, L.cut_skip, src);
+    M.bxv = __shfl_sync(0xffffffffu, L.bxv, src);
+    M.byv = __shfl_sync(0xffffffffu, L.byv, src);
     if (OP != kMap) {
         M.xc = __shfl_sync(0xffffffffu, L.xc, src);
         M.yc = __shfl_sync(0xffffffffu, L.yc, src);
@@ -578,13 +655,23 @@ __device__ __forceinline__ LorConst shfl_lor(const LorConst &L, int src) {
     return M;
 }
 
-// Shared-memory slab layout: rows padded to gx + 1 floats and slices to a stride that
-// is 5 (mod 32) floats, so that a warp's lanes — often consecutive slices of one LOR at
-// the same (row, column), or different LORs in one row — fall into different banks.
-__host__ __device__ __forceinline__ int slab_row_stride(int gx) { return gx + 1; }
-__host__ __device__ __forceinline__ int slab_slice_stride(int gx, int gy) {
-    const int dense = gy * (gx + 1);
+// Shared-memory slab layout. Every slice of the slab has pad = P - 1 zero rows and
+// columns around it, so a window that meets the grid never leaves the slab: row iy,
+// column ix of slab slice sl sits at origin + sl * ss + iy * rs + ix with rs = gx + pad
+// (a row's right padding is the next row's left padding) and pad rows between slices
+// (the bottom padding of one slice is the top padding of the next). The slice stride is
+// rounded up to 5 (mod 32) floats so that a warp's lanes, often consecutive slices of
+// one LOR at the same (row, column), fall into different banks.
+__host__ __device__ __forceinline__ int slab_row_stride(int gx, int pad) { return gx + pad; }
+__host__ __device__ __forceinline__ int slab_slice_stride(int gx, int gy, int pad) {
+    const int dense = (gy + pad) * (gx + pad);
     return dense + ((5 - dense % 32) + 32) % 32;
+}
+__host__ __device__ __forceinline__ int slab_origin(int gx, int pad) {
+    return pad * (gx + pad) + pad;
+}
+__host__ __device__ __forceinline__ int slab_floats(int nsl, int gx, int gy, int pad) {
+    return nsl * slab_slice_stride(gx, gy, pad) + slab_origin(gx, pad);
 }
 
 template <int OP, int P>
@@ -594,11 +681,19 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int kWarps = kSlabThreads / 32;
     const int slice_mesh = p.gx * p.gy;
-    const int rs = slab_row_stride(p.gx), ss = slab_slice_stride(p.gx, p.gy);
+    constexpr int pad = P - 1;
+    const int rs = slab_row_stride(p.gx, pad), ss = slab_slice_stride(p.gx, p.gy, pad);
+    const int origin = slab_origin(p.gx, pad);
     const int64_t total = sp.slab_offs[sp.n_slabs];
     const int64_t g = blockIdx.x, G = gridDim.x;
     const int64_t lo = total * g / G, hi = total * (g + 1) / G;
     if (lo >= hi) return;
+    if (OP == kProj) {
+        // The padding stays zero: the slab loads below write grid voxels only.
+        const int n = slab_floats(sp.nsl, p.gx, p.gy, pad);
+        for (int i = threadIdx.x; i < n; i += kSlabThreads) slab[i] = 0.0f;
+        __syncthreads();
+    }
     int k = 0;
     {
         int a = 0, b = sp.n_slabs - 1;
@@ -622,11 +717,12 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
             for (int r = warp; r < n_rows; r += kWarps) {
                 const int sl = r / p.gy, iy = r - sl * p.gy;
                 const float *g = src + (int64_t)r * p.gx;
-                float *d = slab + sl * ss + iy * rs;
+                float *d = slab + origin + sl * ss + iy * rs;
                 for (int ix = lane; ix < p.gx; ix += 32) d[ix] = __ldg(g + ix);
             }
         } else {
-            for (int i = threadIdx.x; i < (S1 - S0) * ss; i += kSlabThreads) slab[i] = 0.0f;
+            const int n = slab_floats(S1 - S0, p.gx, p.gy, pad);
+            for (int i = threadIdx.x; i < n; i += kSlabThreads) slab[i] = 0.0f;
         }
         __syncthreads();
         for (int64_t q0 = pos + (int64_t)warp * 32; q0 < end; q0 += (int64_t)kWarps * 32) {
@@ -663,16 +759,17 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                 float partial = 0.0f;
                 if (valid) {
                     const int s = a_o + (item - excl_o);
-                    const int off = (s - S0) * ss;
+                    float *sb = slab + origin + (s - S0) * ss;
                     if (OP == kProj) {
                         float acc = 0.0f;
-                        slice_visit<OP, P>(p, M, s, [&](int idx, int iy, float w) {
-                            acc = fmaf(w, slab[off + idx + iy], acc);
+                        slice_visit<OP, P, true>(p, M, s, [&](int ix, int iy, float w, bool use) {
+                            const float v = sb[iy * rs + ix];
+                            acc = use ? fmaf(w, v, acc) : acc;
                         });
                         partial = acc * M.scale;
                     } else {
-                        slice_visit<OP, P>(p, M, s, [&](int idx, int iy, float w) {
-                            atomicAdd(&slab[off + idx + iy], w * M.scale);
+                        slice_visit<OP, P, true>(p, M, s, [&](int ix, int iy, float w, bool use) {
+                            if (use) atomicAdd(&sb[iy * rs + ix], w * M.scale);
                         });
                     }
                 }
@@ -696,7 +793,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
             float *out = p.image_out + img0 + (int64_t)S0 * slice_mesh;
             for (int r = warp; r < n_rows; r += kWarps) {
                 const int sl = r / p.gy, iy = r - sl * p.gy;
-                const float *src = slab + sl * ss + iy * rs;
+                const float *src = slab + origin + sl * ss + iy * rs;
                 float *g = out + (int64_t)r * p.gx;
                 for (int ix = lane; ix < p.gx; ix += 32) {
                     const float v = src[ix];
@@ -752,6 +849,12 @@ int tor_setup(TorParams &p, const int *grid, const float *center, const float *s
                             : -0.5 * log2e / tsc);
     p.tof_scale = p.tof_on ? (float)((double)tof_bin / std::sqrt(2.0 * M_PI * (double)tof_sigma2))
                            : 1.0f;
+    p.inv_x = 1.0f / p.inter_x;
+    p.inv_y = 1.0f / p.inter_y;
+    // |dx|, |dy| <= patch * inter inside a window; the float d^2 of such a voxel is within
+    // ~1e-6 (patch * inter)^2 of the exact value, the margin is 2^-16 (patch * inter)^2.
+    const float span = (float)p.patch * std::max(p.inter_x, p.inter_y);
+    p.box_e = span * span * (1.0f / 65536.0f);
     p.n = n;
     p.stride = lor_stride;
     // Kernel family: the shared-memory slab kernels unless tuning selects the LOR-centric
@@ -767,12 +870,13 @@ void launch_p(const TorParams &p, int grid, int block, cudaStream_t stream) {
 
 // Slices per slab (as many as fit in shared memory) and slab count; false when one
 // slice does not fit (the global-atomics kernel is used then).
-bool slab_geometry(const TorParams &p, int &nsl, int &n_slabs) {
-    if (p.gx > (1 << 15) || p.gy > (1 << 15)) return false;
-    const size_t slice_bytes = sizeof(float) * (size_t)slab_slice_stride(p.gx, p.gy);
-    const size_t budget = kSlabSmemBytes;
-    if (slice_bytes > budget) return false;
-    nsl = (int)std::min<size_t>(budget / slice_bytes, (size_t)p.gz);
+bool slab_geometry(const TorParams &p, int pad, int &nsl, int &n_slabs) {
+    if (p.gx > (1 << 14) || p.gy > (1 << 14)) return false;
+    const size_t slice_floats = (size_t)slab_slice_stride(p.gx, p.gy, pad);
+    const size_t fixed = (size_t)slab_origin(p.gx, pad);
+    const size_t budget = kSlabSmemBytes / sizeof(float);
+    if (slice_floats + fixed > budget) return false;
+    nsl = (int)std::min<size_t>((budget - fixed) / slice_floats, (size_t)p.gz);
     const int want = g_tune_nsl.load(std::memory_order_relaxed);
     if (want > 0) nsl = std::min(nsl, want);
     n_slabs = (p.gz + nsl - 1) / nsl;
@@ -782,7 +886,7 @@ bool slab_geometry(const TorParams &p, int &nsl, int &n_slabs) {
 template <int OP, int P>
 int launch_slab(const TorParams &p, cudaStream_t stream) {
     SegPlan sp{};
-    if (!slab_geometry(p, sp.nsl, sp.slabs_pf)) return -1;
+    if (!slab_geometry(p, P - 1, sp.nsl, sp.slabs_pf)) return -1;
     sp.n_slabs = sp.slabs_pf * std::max(1, p.n_frames);
     sp.ntiles = (int)((p.n + kSegTile - 1) / kSegTile);
     // Scratch from the stream-ordered pool: no host synchronisation, capturable. The
@@ -822,7 +926,7 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
         }
         attr_set.fetch_or(1ull << dev);
     }
-    const size_t smem = sizeof(float) * (size_t)sp.nsl * slab_slice_stride(p.gx, p.gy);
+    const size_t smem = sizeof(float) * (size_t)slab_floats(sp.nsl, p.gx, p.gy, P - 1);
     int64_t *slab_tot = sp.slab_offs + sp.n_slabs + 1;
     if (OP == kProj) {
         e = cudaMemsetAsync(p.proj_out, 0, sizeof(float) * p.n, stream);
