@@ -62,6 +62,9 @@ def parse_args(argv=None):
                     help="tor128: the headline TOF-TOR pair (default); batched96: 64-frame "
                          "batched OSEM iteration vs the plain per-frame loop")
     ap.add_argument("--frames", type=int, default=64)
+    ap.add_argument("--tuning", default=None,
+                    help="PATH,SLAB_SLICES,GRID_MULT for srf_tor_set_tuning (default: the "
+                         "library's automatic choice)")
     return ap.parse_args(argv)
 
 
@@ -184,6 +187,31 @@ def algorithmic_work(model, data, image):
         per[a] = {"lors": int(cnt.shape[1]), "useful": int(cnt[0].sum(dtype=torch.int64)),
                   "slots": int(cnt[1].sum(dtype=torch.int64))}
     return per
+
+
+def roofline_components(kernel, ms_per_step, alg_bytes, n_lors, rec, useful, slots, hbm_peak,
+                        probe):
+    """Bound time of the dominant op per step as the slowest of three measured limits:
+    HBM (algorithmic bytes / measured copy bandwidth), L2 (the same bytes / the measured
+    L2 read bandwidth) and SFU (one exp per non-zero-weight sample / measured ex2 rate);
+    frac = bound / measured. The reference's own exp count (one TOF exp per window
+    sample plus one geometric exp per non-zero sample) is given for comparison."""
+    t_hbm = alg_bytes / (hbm_peak * 1e9)
+    t_l2 = alg_bytes / (probe["l2_gbs"] * 1e9)
+    t_sfu = useful / probe["ex2_per_s"]
+    t_meas = ms_per_step / 1e3
+    bound = max(t_hbm, t_l2, t_sfu)
+    per = 8 if kernel == "srf_tor_backprojection" else 4
+    return {
+        "hbm": {"ms": t_hbm * 1e3, "frac": t_hbm / t_meas, "peak_gbs": hbm_peak},
+        "l2": {"ms": t_l2 * 1e3, "frac": t_l2 / t_meas, "peak_gbs": probe["l2_gbs"]},
+        "sfu": {"ms": t_sfu * 1e3, "frac": t_sfu / t_meas, "peak_ex2_per_s": probe["ex2_per_s"],
+                "exps": useful, "reference_exps": useful + slots},
+        "bound_ms": bound * 1e3, "measured_ms": ms_per_step, "frac_of_bound": bound / t_meas,
+        "window_sample_bytes": n_lors * (rec + 4) + per * slots,
+        "window_sample_frac_hbm": (n_lors * (rec + 4) + per * slots) / (hbm_peak * 1e9) / t_meas,
+        "probe": probe["method"],
+    }
 
 
 # ------------------------------------------------------------------ CPU baseline
@@ -407,6 +435,9 @@ def main(argv=None):
     from srf_b200 import Image, backprojection, projection, profiling
     from srf_b200 import preprocess as PP
 
+    if args.tuning:
+        from srf_b200 import tuning
+        tuning.set_tuning(*[int(v) for v in args.tuning.split(",")])
     wl, events, img_np, tof_bin, tof_sigma2 = workload_inputs(args.events, rank, dev)
     n_events = events.shape[0]
     model = model_for(wl, tof_bin, tof_sigma2)
@@ -434,6 +465,8 @@ def main(argv=None):
     if clocks:
         clocks.start()
     timer = profiling.KernelTimer()
+    from srf_b200 import _lib
+    launches0 = _lib.call_raw("srf_launch_count")
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("bench_timed")
     with timer:
@@ -442,6 +475,7 @@ def main(argv=None):
             step()
         end.record()
     torch.cuda.nvtx.range_pop()
+    gpu_launches = _lib.call_raw("srf_launch_count") - launches0
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
@@ -495,10 +529,12 @@ def main(argv=None):
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     useful = sum(w["useful"] for w in work.values())
+    slots = sum(w["slots"] for w in work.values())
     rec = 40  # bytes of one preprocessed LOR record (10 float32)
     alg = {"srf_tor_projection": n_lors * (rec + 4) + 4 * useful,
            "srf_tor_backprojection": n_lors * (rec + 4) + 8 * useful}
     roof = None
+    peaks_probe = profiling.measure_peaks() if kern else None
     if kern:
         dom = max(kern, key=lambda k: kern[k]["total_ms"])
         launches = kern[dom]["launches"]
@@ -513,6 +549,10 @@ def main(argv=None):
                 "peak_source": f"{peak_src} hbm_gbs (burst copy)",
                 "algorithmic_bytes_per_launch": per_launch_bytes,
                 "useful_samples_per_step": useful,
+                "window_samples_per_step": slots,
+                "components": roofline_components(dom, kern[dom]["total_ms"] / args.steps,
+                                                  alg[dom], n_lors, rec, useful, slots,
+                                                  hbm_peak, peaks_probe),
                 "kernel_ms": {k: {"launches": v["launches"], "mean_ms": v["mean_ms"],
                                   "share": v["total_ms"] / sum(x["total_ms"] for x in kern.values())}
                               for k, v in kern.items()}}
@@ -526,7 +566,6 @@ def main(argv=None):
             base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
                     "sample": f"unavailable: {exc}"}
 
-    gpu_launches = sum(v["launches"] for v in kern.values())
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
@@ -538,7 +577,8 @@ def main(argv=None):
                            "tof_bin_mm": tof_bin, "tof_sigma2": tof_sigma2,
                            "groups": {a: w["lors"] for a, w in work.items()},
                            "parallelism": f"events sharded, {world} rank(s)",
-                           "l2": "inputs larger than L2 (400 MB LOR records per rank)"},
+                           "l2": "inputs larger than L2 (400 MB LOR records per rank)",
+                           "tuning": args.tuning or "automatic"},
                 "roofline": roof, "cpu_baseline": base, "e2e": e2e,
                 "gpu_launches": gpu_launches, "clocks": clk}
         print(json.dumps(line), flush=True)

@@ -41,6 +41,14 @@ typedef enum {
 const char *srf_status_string(int status);
 int srf_last_cuda_error(void);
 int srf_version(void);
+/* Number of kernels this library has launched in this process (all devices, all entry
+ * points); a caller diffs it around a region to count that region's launches. */
+int64_t srf_launch_count(void);
+/* The TOR slab kernels take stream-ordered scratch (the per-slab LOR lists, up to
+ * 4 bytes x LORs x slabs per frame) from a memory pool the library keeps per device;
+ * the pool retains its memory between calls. This returns all of it that is not in use
+ * to the driver. */
+int srf_release_scratch(void);
 
 /* ------------------------------------------------------------------ TOR (tube of response)
  * Field columns for TOR: x1,y1,z1,x2,y2,z2 (LOR endpoints, dominant axis last, as
@@ -138,7 +146,8 @@ int srf_tor_backproject_adjoint_batched(const float *x1, const float *y1, const 
 
 /* No counterpart in the reference: process-wide tuning of the TOR kernels (used by the
  * autotuner; affects later calls from every thread). path: 0 automatic, 1 shared-memory
- * slab kernels, 2 LOR-centric kernels (L2 gathers, global atomics); slab_slices: slices
+ * slab kernels with one lane per (LOR, slab) segment, 2 LOR-centric kernels (L2 gathers,
+ * global atomics), 3 slab kernels with a segment's slices spread over lanes; slab_slices: slices
  * per slab, 0 = as many as fit; grid_mult: persistent slab CTAs = SMs x grid_mult (1..8). */
 int srf_tor_set_tuning(int path, int slab_slices, int grid_mult);
 
@@ -232,6 +241,19 @@ int srf_map_process(const float *lors, int64_t num_lors, int64_t lor_stride, flo
 /* MLEM/OSEM update of model/recon_step.py:48-49: image[v] *= effinv[v] * bp[v]. */
 int srf_mlem_update(float *image, const float *effinv, const float *bp, int64_t num_voxels,
                     void *stream);
+
+/* ------------------------------------------------------------------------ peak probes */
+
+/* No counterpart in the reference: measurement kernels for the roofline denominators
+ * that are not a plain HBM copy, timed by the caller with events on `stream`.
+ * srf_probe_threads: threads per probe launch (the length of `sink` in floats).
+ * srf_probe_l2_read: every thread reads a 16-byte-aligned buffer of n_floats (sized to
+ *   stay L2-resident) `reps` times with L2-only loads; bytes read = reps * 4 * n_floats
+ *   rounded down to 16-byte vectors.
+ * srf_probe_ex2: every thread evaluates 8 * iters dependent-by-chain ex2.approx. */
+int srf_probe_threads(int64_t *n_threads);
+int srf_probe_l2_read(const float *buf, int64_t n_floats, int reps, float *sink, void *stream);
+int srf_probe_ex2(int iters, float *sink, void *stream);
 
 #ifdef __cplusplus
 }

@@ -23,6 +23,8 @@ SIGNATURES = {
     "srf_status_string": ([_int], C.c_char_p),
     "srf_last_cuda_error": ([], _int),
     "srf_version": ([], _int),
+    "srf_launch_count": ([], _i64),
+    "srf_release_scratch": ([], _int),
     "srf_tor_projection": (_TOR_COLS + [_int, _p, _p, _p, _p, _f, _f, _f, _p, _i64, _i64, _p],
                            _int),
     "srf_tor_backprojection": (_TOR_COLS + [_int, _p, _p, _p, _p, _f, _f, _f, _p, _i64, _i64,
@@ -50,6 +52,9 @@ SIGNATURES = {
     "srf_recon_process": ([_p, _i64, _i64, C.c_double, _p, _p, _p, _i64, _p], _int),
     "srf_map_process": ([_p, _i64, _i64, _p, _p, _p, _i64, _p], _int),
     "srf_recon_process_noalloc": ([_p, _i64, _i64, C.c_double, _p, _p, _p], _int),
+    "srf_probe_threads": ([_p], _int),
+    "srf_probe_l2_read": ([_p, _i64, _int, _p, _p], _int),
+    "srf_probe_ex2": ([_int, _p, _p], _int),
 }
 
 
@@ -97,6 +102,11 @@ def call(name, *args):
     if st != 0:
         raise SRFError(name, st, lib)
     return st
+
+
+def call_raw(name, *args):
+    """Call an entry point that returns a value rather than a status."""
+    return getattr(load(), name)(*args)
 
 
 def exported_symbols():

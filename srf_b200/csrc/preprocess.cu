@@ -312,10 +312,12 @@ int preprocess(const float *events, int64_t n, int64_t stride, int recon, double
         classify_kernel<true><<<p.ntiles, kThreads, 0, stream>>>(p);
         scan_kernel<<<1, 1024, 0, stream>>>(p);
         scatter_kernel<true><<<p.ntiles, kThreads, 0, stream>>>(p);
+        count_launches(3);
     } else {
         classify_kernel<false><<<p.ntiles, kThreads, 0, stream>>>(p);
         scan_kernel<<<1, 1024, 0, stream>>>(p);
         scatter_kernel<false><<<p.ntiles, kThreads, 0, stream>>>(p);
+        count_launches(3);
     }
     return check_launch();
 }

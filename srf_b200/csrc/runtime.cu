@@ -15,9 +15,44 @@ namespace {
 thread_local int g_last_cuda_error = 0;
 constexpr int kMaxDevices = 64;
 std::atomic<int> g_sms[kMaxDevices];
+std::atomic<long long> g_launches{0};
 }  // namespace
 
 void set_cuda_error(cudaError_t e) { g_last_cuda_error = (int)e; }
+
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+}  // namespace
+
+cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaMallocAsync(ptr, bytes, stream);
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        if (!g_pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&g_pools[dev], &props);
+            if (e != cudaSuccess) {
+                g_pools[dev] = nullptr;
+                return e;
+            }
+            uint64_t keep = UINT64_MAX;
+            e = cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+            if (e != cudaSuccess) return e;
+        }
+        pool = g_pools[dev];
+    }
+    return cudaMallocFromPoolAsync(ptr, bytes, pool, stream);
+}
 
 int num_sms() {
     int dev = 0;
@@ -77,6 +112,23 @@ extern "C" int srf_last_cuda_error(void) { return g_last_cuda_error; }
 
 extern "C" int srf_version(void) { return 1; }
 
+extern "C" int srf_release_scratch(void) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    for (int d = 0; d < kMaxDevices; d++) {
+        if (!g_pools[d]) continue;
+        cudaError_t e = cudaMemPoolTrimTo(g_pools[d], 0);
+        if (e != cudaSuccess) {
+            set_cuda_error(e);
+            return SRF_ERR_CUDA;
+        }
+    }
+    return SRF_OK;
+}
+
+extern "C" int64_t srf_launch_count(void) {
+    return (int64_t)g_launches.load(std::memory_order_relaxed);
+}
+
 extern "C" int srf_mlem_update(float *image, const float *effinv, const float *bp,
                                int64_t num_voxels, void *stream) {
     if (num_voxels < 0) return SRF_ERR_INVALID_ARGUMENT;
@@ -85,5 +137,6 @@ extern "C" int srf_mlem_update(float *image, const float *effinv, const float *b
     const int block = 256;
     const int grid = stride_grid((num_voxels + 3) / 4, block, 4);
     mlem_update_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(image, effinv, bp, num_voxels);
+    count_launches(1);
     return check_launch();
 }

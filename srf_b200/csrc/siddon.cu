@@ -231,6 +231,7 @@ int siddon_launch(const SiddonParams &p, cudaStream_t stream) {
     const int block = 256;
     const int grid = stride_grid(p.n, block, 8);
     siddon_kernel<OP><<<grid, block, 0, stream>>>(p);
+    count_launches(1);
     return check_launch();
 }
 

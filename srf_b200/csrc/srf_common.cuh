@@ -37,6 +37,16 @@ inline int check_launch() {
 
 int num_sms();
 
+// Stream-ordered scratch from the library's own memory pool on the current device. The
+// pool keeps what it has reserved across calls (release threshold: never), so repeated
+// calls of the same size neither map nor unmap device memory; srf_release_scratch()
+// returns it. Allocation and free are capturable in CUDA graphs.
+cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream);
+
+// Process-wide count of kernels this library has launched (srf_launch_count); every
+// launch site adds its launches.
+void count_launches(int n);
+
 // Grid for a grid-stride kernel: enough blocks to fill every SM `per_sm` times, but
 // no more than the work needs.
 inline int stride_grid(int64_t work_items, int items_per_block, int per_sm) {

@@ -33,7 +33,8 @@ namespace {
 
 enum TorOp { kProj = 0, kBack = 1, kMap = 2, kAdj = 3, kCount = 4 };
 
-// Process-wide tuning (srf_tor_set_tuning): kernel family (0 auto, 1 slab, 2 LOR-centric),
+// Process-wide tuning (srf_tor_set_tuning): kernel family (0 auto, 1 slab with a lane per
+// segment, 2 LOR-centric, 3 slab with items spread over lanes),
 // slices per slab (0 = as many as fit), grid multiplier of the persistent slab kernel
 // (CTAs = SMs x mult, one resident per SM: more, smaller shares of the segment list).
 std::atomic<int> g_tune_path{0};
@@ -61,6 +62,7 @@ struct TorParams {
     float *proj_out;
     int *count_out;   // kCount: [n] voxels with non-zero weight, [n] window voxels visited
     int use_slab;     // scatter ops: shared-memory slab kernel (1) or global atomics (0)
+    int slab_expand;  // slab kernel: spread items over lanes (1) or a lane per segment (0)
     // Batched frames: LOR i belongs to frame frame[i] (null: one frame) whose image starts
     // frame_stride floats after the previous frame's.
     const int *frame;
@@ -318,6 +320,16 @@ __device__ __forceinline__ bool lor_slices(const TorParams &p, int64_t t, int &s
     return s_lo <= s_hi;
 }
 
+// (int)(a / b) with a correctly rounded quotient, as the reference truncates it
+// (tor.cu.cc:135-136). q = a * (1/b) is within 2^-22 |a/b| of the rounded quotient, so
+// both truncate to the same integer unless q lies that close to an integer (or is 0);
+// only then is the division itself evaluated.
+__device__ __forceinline__ int trunc_div(float a, float b, float inv_b) {
+    const float q = a * inv_b;
+    if (fabsf(q - rintf(q)) <= fabsf(q) * 1.0e-6f) return __float2int_rz(__fdiv_rn(a, b));
+    return __float2int_rz(q);
+}
+
 // One voxel slot: the reference's d^2 (tor.cu.cc:61-66, FMA-contracted as nvcc builds
 // it) and cut-off decision, and the folded exponent.
 template <int OP, typename F>
@@ -375,8 +387,8 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
     const float cx = __fmaf_rn(L.d0, ratio, L.x1);
     const float cy = __fmaf_rn(L.d1, ratio, L.y1);
     const float rx = __fsub_rn(cx, p.l_bound), ry = __fsub_rn(cy, p.b_bound);
-    const int ix0 = __float2int_rz(__fdiv_rn(rx, p.inter_x)) - p.half;
-    const int iy0 = __float2int_rz(__fdiv_rn(ry, p.inter_y)) - p.half;
+    const int ix0 = trunc_div(rx, p.inter_x, p.inv_x) - p.half;
+    const int iy0 = trunc_div(ry, p.inter_y, p.inv_y) - p.half;
     if (ix0 >= p.gx || iy0 >= p.gy || ix0 <= -P || iy0 <= -P) return 0;  // window off the grid
     int n_slots = 0;
     if (OP == kCount) {
@@ -420,14 +432,26 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
         dxs[i] = __fsub_rn(cx, mxi);
     }
     if (kPadded) {
-        // wx, wy are warp-uniform: one fully unrolled row body per width, so that the
-        // row's loads issue back to back.
-        for (int j = 0; j < wy; j++) {
-            const int iy = ylo + j;
-            const float dy = __fsub_rn(cy, __fmaf_rn(p.inter_y, (float)iy + 0.5f, p.b_bound));
+        // wx, wy are warp-uniform: one fully unrolled row body per width, so that a row's
+        // loads issue back to back. The gather picks the body once per slice; the scatter
+        // (a compare-and-swap loop per voxel in shared memory) runs faster picking it per
+        // row (measured).
+        const float fy0 = (float)ylo + 0.5f;
+        if (OP == kProj) {
             with_width<P>(wx, [&](auto W) {
-                row_slots<OP, decltype(W)::value>(L, dxs, dy, k0, xlo, iy, f);
+                for (int j = 0; j < wy; j++) {
+                    const float dy =
+                        __fsub_rn(cy, __fmaf_rn(p.inter_y, fy0 + (float)j, p.b_bound));
+                    row_slots<OP, decltype(W)::value>(L, dxs, dy, k0, xlo, ylo + j, f);
+                }
             });
+        } else {
+            for (int j = 0; j < wy; j++) {
+                const float dy = __fsub_rn(cy, __fmaf_rn(p.inter_y, fy0 + (float)j, p.b_bound));
+                with_width<P>(wx, [&](auto W) {
+                    row_slots<OP, decltype(W)::value>(L, dxs, dy, k0, xlo, ylo + j, f);
+                });
+            }
         }
     } else {
 #pragma unroll
@@ -674,7 +698,10 @@ __host__ __device__ __forceinline__ int slab_floats(int nsl, int gx, int gy, int
     return nsl * slab_slice_stride(gx, gy, pad) + slab_origin(gx, pad);
 }
 
-template <int OP, int P>
+// kExpand: the (LOR, slice) items of a warp's 32 segments are spread over its lanes, 32
+// at a time (one item per lane, LOR constants shuffled to it); otherwise each lane walks
+// its own segment's slices.
+template <int OP, int P, bool kExpand>
 __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorParams p, SegPlan sp) {
     extern __shared__ float slab[];
     __shared__ signed char owner_tab[kSlabThreads / 32][32];
@@ -735,6 +762,25 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                     a = max(L.s_lo, S0);
                     cnt = max(0, min(L.s_hi, S1 - 1) - a + 1);
                 }
+            }
+            if (!kExpand) {
+                float acc = 0.0f;
+                for (int i = 0; i < cnt; i++) {
+                    const int s = a + i;
+                    float *sb = slab + origin + (s - S0) * ss;
+                    if (OP == kProj) {
+                        slice_visit<OP, P, true>(p, L, s, [&](int ix, int iy, float w, bool use) {
+                            const float v = sb[iy * rs + ix];
+                            acc = use ? fmaf(w, v, acc) : acc;
+                        });
+                    } else {
+                        slice_visit<OP, P, true>(p, L, s, [&](int ix, int iy, float w, bool use) {
+                            if (use) atomicAdd(&sb[iy * rs + ix], w * L.scale);
+                        });
+                    }
+                }
+                if (OP == kProj && cnt > 0) atomicAdd(p.proj_out + t, acc * L.scale);
+                continue;
             }
             int incl = cnt;
 #pragma unroll
@@ -859,13 +905,16 @@ int tor_setup(TorParams &p, const int *grid, const float *center, const float *s
     p.stride = lor_stride;
     // Kernel family: the shared-memory slab kernels unless tuning selects the LOR-centric
     // ones (gathers from L2, global atomics; also the fallback when a slice does not fit).
-    p.use_slab = g_tune_path.load(std::memory_order_relaxed) == 2 ? 0 : 1;
+    const int path = g_tune_path.load(std::memory_order_relaxed);
+    p.use_slab = path == 2 ? 0 : 1;
+    p.slab_expand = path == 3 ? 1 : 0;
     return SRF_OK;
 }
 
 template <int OP, int P>
 void launch_p(const TorParams &p, int grid, int block, cudaStream_t stream) {
     tor_kernel_p<OP, P><<<grid, block, 0, stream>>>(p);
+    count_launches(1);
 }
 
 // Slices per slab (as many as fit in shared memory) and slab count; false when one
@@ -889,8 +938,9 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
     if (!slab_geometry(p, P - 1, sp.nsl, sp.slabs_pf)) return -1;
     sp.n_slabs = sp.slabs_pf * std::max(1, p.n_frames);
     sp.ntiles = (int)((p.n + kSegTile - 1) / kSegTile);
-    // Scratch from the stream-ordered pool: no host synchronisation, capturable. The
-    // segment list is sized for the worst case (every LOR in every slab it can reach).
+    // Scratch from the library's stream-ordered pool: no host synchronisation,
+    // capturable. The segment list is sized for the worst case (every LOR in every slab
+    // it can reach).
     const int64_t max_slabs_per_lor = sp.slabs_pf;
     const size_t cap = (size_t)p.n * (size_t)max_slabs_per_lor;
     auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
@@ -900,8 +950,8 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
     const size_t b_slab = al(sizeof(int64_t) * (2 * sp.n_slabs + 1));
     const size_t b_seg = al(sizeof(int) * cap);
     char *ws = nullptr;
-    cudaError_t e = cudaMallocAsync((void **)&ws, b_range + b_counts + b_offs + b_slab + b_seg,
-                                    stream);
+    cudaError_t e = scratch_alloc((void **)&ws, b_range + b_counts + b_offs + b_slab + b_seg,
+                                  stream);
     if (e != cudaSuccess) {
         set_cuda_error(e);
         return SRF_ERR_CUDA;
@@ -912,19 +962,21 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
     sp.slab_offs = reinterpret_cast<int64_t *>(ws + b_range + b_counts + b_offs);
     sp.seg = reinterpret_cast<int *>(ws + b_range + b_counts + b_offs + b_slab);
 
-    static std::atomic<unsigned long long> attr_set{0};  // per template instance, per device
+    void (*kern)(const TorParams, SegPlan) =
+        p.slab_expand ? tor_slab_kernel<OP, P, true> : tor_slab_kernel<OP, P, false>;
+    static std::atomic<unsigned long long> attr_set[2];  // per kernel instance, per device
+    std::atomic<unsigned long long> &done = attr_set[p.slab_expand ? 1 : 0];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
-    if (!(attr_set.load() & (1ull << dev))) {
-        e = cudaFuncSetAttribute(tor_slab_kernel<OP, P>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (!(done.load() & (1ull << dev))) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSlabSmemBytes);
         if (e != cudaSuccess) {
             set_cuda_error(e);
             cudaFreeAsync(ws, stream);
             return SRF_ERR_CUDA;
         }
-        attr_set.fetch_or(1ull << dev);
+        done.fetch_or(1ull << dev);
     }
     const size_t smem = sizeof(float) * (size_t)slab_floats(sp.nsl, p.gx, p.gy, P - 1);
     int64_t *slab_tot = sp.slab_offs + sp.n_slabs + 1;
@@ -941,7 +993,8 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
     seg_offsets_kernel<<<1, 32, 0, stream>>>(sp, slab_tot);
     seg_fill_kernel<<<sp.ntiles, kSegThreads, 0, stream>>>(p, sp);
     const int mult = std::max(1, std::min(8, g_tune_mult.load(std::memory_order_relaxed)));
-    tor_slab_kernel<OP, P><<<num_sms() * mult, kSlabThreads, smem, stream>>>(p, sp);
+    kern<<<num_sms() * mult, kSlabThreads, smem, stream>>>(p, sp);
+    count_launches(5);
     int st = check_launch();
     e = cudaFreeAsync(ws, stream);
     if (st == SRF_OK && e != cudaSuccess) {
@@ -978,7 +1031,10 @@ int tor_launch(TorParams &p, cudaStream_t stream, bool generic = false) {
         case 6: launch_p<OP, 6>(p, grid, block, stream); break;
         case 7: launch_p<OP, 7>(p, grid, block, stream); break;
         case 8: launch_p<OP, 8>(p, grid, block, stream); break;
-        default: tor_kernel<OP><<<grid, block, 0, stream>>>(p); break;
+        default:
+            tor_kernel<OP><<<grid, block, 0, stream>>>(p);
+            count_launches(1);
+            break;
     }
     return check_launch();
 }
@@ -1237,7 +1293,7 @@ extern "C" int srf_tor_backproject_adjoint_batched(
 // 1 slab kernels, 2 LOR-centric kernels; slab_slices: slices per shared-memory slab
 // (0 = as many as fit); grid_mult: persistent slab CTAs = SMs x grid_mult (1..8).
 extern "C" int srf_tor_set_tuning(int path, int slab_slices, int grid_mult) {
-    if (path < 0 || path > 2 || slab_slices < 0 || grid_mult < 1 || grid_mult > 8)
+    if (path < 0 || path > 3 || slab_slices < 0 || grid_mult < 1 || grid_mult > 8)
         return SRF_ERR_INVALID_ARGUMENT;
     g_tune_path.store(path);
     g_tune_nsl.store(slab_slices);

@@ -63,3 +63,37 @@ def timed_call(name, stream):
         torch.cuda.nvtx.range_pop()
         e.record(stream)
         t.records.append((name, s, e))
+
+
+def measure_peaks(device=None, l2_mib=48, l2_reps=20, ex2_iters=4096):
+    """Measured L2 read bandwidth (GB/s) and ex2 throughput (per second) of this GPU,
+    from the library's probe kernels (``srf_probe_l2_read``, ``srf_probe_ex2``): one
+    warm-up and one timed launch each, CUDA events on the current stream. The L2 buffer
+    (default 48 MiB) stays resident in the 126 MB L2."""
+    import ctypes
+
+    from . import _lib
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    with torch.cuda.device(dev):
+        nt = ctypes.c_int64(0)
+        _lib.call("srf_probe_threads", ctypes.byref(nt))
+        sink = torch.empty(nt.value, dtype=torch.float32, device=dev)
+        n = l2_mib * (1 << 20) // 4
+        buf = torch.rand(n, dtype=torch.float32, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def timed(fn):
+            fn()
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize(dev)
+            return s.elapsed_time(e) / 1e3
+
+        t_l2 = timed(lambda: _lib.call("srf_probe_l2_read", buf.data_ptr(), n, l2_reps,
+                                       sink.data_ptr(), stream))
+        t_ex2 = timed(lambda: _lib.call("srf_probe_ex2", ex2_iters, sink.data_ptr(), stream))
+    l2_bytes = l2_reps * (n // 4) * 16
+    return {"l2_gbs": l2_bytes / t_l2 / 1e9, "ex2_per_s": nt.value * 8 * ex2_iters / t_ex2,
+            "l2_buffer_mib": l2_mib, "method": "srf_probe_l2_read / srf_probe_ex2, CUDA events"}

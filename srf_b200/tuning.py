@@ -1,8 +1,9 @@
 """Kernel tuning for the TOR ops and a small autotuner.
 
 ``set_tuning(path, slab_slices, grid_mult)`` sets the library's process-wide knobs
-(``srf_tor_set_tuning``): the kernel family (0 automatic, 1 shared-memory slabs,
-2 LOR-centric), the number of slices per shared-memory slab (0 = as many as fit) and
+(``srf_tor_set_tuning``): the kernel family (0 automatic, 1 shared-memory slabs with a
+lane per (LOR, slab) segment, 2 LOR-centric, 3 shared-memory slabs with a segment's
+slices spread over lanes), the number of slices per shared-memory slab (0 = as many as fit) and
 the grid multiplier of the persistent slab kernel.
 
 ``Autotuner`` times a caller-supplied step (for example one OSEM sub-iteration on a
@@ -28,13 +29,13 @@ def set_tuning(path=0, slab_slices=0, grid_mult=1):
 
 
 def candidates(max_slab_slices):
-    """Settings worth trying: full and half-depth slabs, grid multipliers 1 and 2, and
-    the LOR-centric kernels."""
+    """Settings worth trying: full and half-depth slabs, grid multipliers 1 and 2, the
+    spread-items slab kernel and the LOR-centric kernels."""
     out = [(1, 0, 1), (1, 0, 2)]
     half = max(1, max_slab_slices // 2)
     if half < max_slab_slices:
         out += [(1, half, 1), (1, half, 2)]
-    out.append((2, 0, 1))
+    out += [(3, 0, 1), (2, 0, 1)]
     return out
 
 

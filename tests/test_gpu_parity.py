@@ -69,14 +69,18 @@ def tcase():
     return K.tor_case(n=3000, seed=31, grid=(128, 128, 64), voxel=3.2, n_box=600)
 
 
-@pytest.fixture(params=["slab", "global"])
+# Tuning paths of the TOR kernels: shared-memory slabs with a lane per (LOR, slab)
+# segment (1, the default), slabs with a segment's slices spread over lanes (3), and
+# LOR-centric kernels reading the image from L2 with global atomics (2, the fallback when
+# a slice does not fit in shared memory).
+TOR_PATHS = {"slab": 1, "slab_spread": 3, "global": 2}
+
+
+@pytest.fixture(params=list(TOR_PATHS))
 def tor_path(request):
-    """The TOR ops have two kernel families: shared-memory slabs (default) and
-    LOR-centric kernels reading the image from L2 with global atomics
-    (tuning path 2, the fallback when a slice does not fit in shared memory).
-    Both must agree with the oracle."""
+    """Every TOR kernel family must agree with the oracle."""
     from srf_b200 import tuning
-    tuning.set_tuning(path=1 if request.param == "slab" else 2)
+    tuning.set_tuning(path=TOR_PATHS[request.param])
     yield request.param
     tuning.set_tuning()
 
@@ -101,13 +105,11 @@ def test_tor_projection(tcase, pname, axis, tor_path):
     assert K.rel_l2(gpu_nc, gpu) <= 1e-6
 
 
-@pytest.fixture(params=["slab", "global"])
+@pytest.fixture(params=list(TOR_PATHS))
 def scatter_kernel(request):
-    """Back-projection / map / adjoint have two kernels: shared-memory slabs (default)
-    and global atomics (tuning path 2, the fallback when a slice does not fit in shared
-    memory). Both must agree with the oracle."""
+    """Back-projection / map / adjoint in every TOR kernel family against the oracle."""
     from srf_b200 import tuning
-    tuning.set_tuning(path=1 if request.param == "slab" else 2)
+    tuning.set_tuning(path=TOR_PATHS[request.param])
     yield request.param
     tuning.set_tuning()
 

@@ -144,7 +144,7 @@ def _frames(n_frames, seed, grid=(48, 48, 24), voxel=6.4):
     return frames, list(grid), size
 
 
-@pytest.mark.parametrize("path", [1, 2])
+@pytest.mark.parametrize("path", [1, 2, 3])
 def test_batched_ops_equal_per_frame(path):
     from srf_b200 import tuning
     tuning.set_tuning(path=path)

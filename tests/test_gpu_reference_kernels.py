@@ -14,7 +14,7 @@ import torch
 from oracle import pyoracle as O
 from srf_b200 import ops
 from tests import _cases as K
-from tests.test_gpu_parity import TOL, cu, host, record
+from tests.test_gpu_parity import TOL, TOR_PATHS, cu, host, record
 
 pytestmark = pytest.mark.gpu
 
@@ -31,10 +31,10 @@ def tcase():
     return K.tor_case(n=20000, seed=51, grid=(128, 128, 64), voxel=3.2, n_box=2000)
 
 
-@pytest.fixture(params=["slab", "global"])
+@pytest.fixture(params=list(TOR_PATHS))
 def tor_path(request):
     from srf_b200 import tuning
-    tuning.set_tuning(path=1 if request.param == "slab" else 2)
+    tuning.set_tuning(path=TOR_PATHS[request.param])
     yield request.param
     tuning.set_tuning()
 
