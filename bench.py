@@ -541,7 +541,7 @@ def main(argv=None):
         per_launch_bytes = alg.get(dom, 0) * args.steps / max(launches, 1)
         achieved = per_launch_bytes / (kern[dom]["mean_ms"] / 1e3) / 1e9
         traffic = None
-        prof = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+        prof = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
         if os.path.exists(prof):
             traffic = json.load(open(prof)).get(dom)
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,

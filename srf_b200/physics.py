@@ -130,6 +130,9 @@ def projection(model, image, data):
             raise TypeError("SplitLoRsModel projects ListModeDataSplit")
         res = {}
         for a in model.AXIS:
+            if data[a].lors.shape[0] == 0:  # nothing to launch
+                res[a] = torch.zeros(0, dtype=torch.float32, device=data[a].lors.device)
+                continue
             img, g, c, s = model.kernel_geometry(image, a)
             res[a] = ops.tor_projection(_lors_of(data[a]), img, g, c, s, model.kernel_width,
                                         model.geo_sigma2_flag, model.tof_bin, model.tof_sigma2,
@@ -148,6 +151,8 @@ def _sum_back(model, parts, image):
     for a, bp in parts:
         back = bp.permute(*model.perm_back(a))
         out = back.clone() if out is None else out.add_(back)
+    if out is None:  # every group empty
+        out = torch.zeros_like(image.data)
     return Image(out.contiguous(), image.center, image.size)
 
 
@@ -158,12 +163,16 @@ def backprojection(model, data, image):
         parts = []
         if isinstance(data, ListModeDataSplitWithoutTOF):
             for a in model.AXIS:
+                if data[a].lors.shape[0] == 0:
+                    continue
                 img, g, c, s = model.kernel_geometry(image, a)
                 parts.append((a, ops.tor_maplors(img, g, c, s, _lors_of(data[a]), data[a].values,
                                                  model.kernel_width, model.geo_sigma2_flag,
                                                  layout="nc")))
         elif isinstance(data, ListModeDataSplit):
             for a in model.AXIS:
+                if data[a].lors.shape[0] == 0:
+                    continue
                 img, g, c, s = model.kernel_geometry(image, a)
                 parts.append((a, ops.tor_backprojection(
                     img, _lors_of(data[a]), data[a].values, g, c, s, model.kernel_width,
@@ -190,6 +199,8 @@ def backproject_adjoint(model, data, image):
     if isinstance(model, SplitLoRsModel):
         parts = []
         for a in model.AXIS:
+            if data[a].lors.shape[0] == 0:
+                continue
             img, g, c, s = model.kernel_geometry(image, a)
             parts.append((a, ops.tor_backproject_adjoint(
                 data[a].values, _lors_of(data[a]), g, c, s, model.kernel_width,
