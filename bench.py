@@ -19,8 +19,11 @@ images are summed with one NCCL all-reduce.
 * ``e2e``: the same metric through the public API from pinned HOST buffers: each step
   copies the raw events host->device, preprocesses them, projects, back-projects and
   copies the image back.
-* ``roofline``: the dominant kernel's algorithmic bytes per launch over its
-  CUDA-event duration inside the timed region (see DESIGN.md for the byte model).
+* ``roofline``: the dominant op's algorithmic bytes per call (per LOR: the 40-byte
+  record, 4 bytes of output or value, and 4 bytes per non-zero-weight voxel sample for
+  the projection, 8 for the back-projection's read-modify-write) over its CUDA-event
+  duration inside the timed region, against the measured HBM copy bandwidth; plus the
+  bound of the slowest of HBM, L2 and SFU (ex2) at their measured peaks.
 * ``cpu_baseline``: the reference's own projector sources compiled for the host
   (oracle/_ref), all host threads, on a bounded sample of the same LORs.
 
@@ -45,6 +48,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "TOF-TOR proj+backproj LORs/s at 128x128x64 (10M events)"
+METRICS = {
+    "tor128": METRIC,
+    "large256": "TOF-TOR proj+backproj LORs/s at 256x256x128 (16M-event chunk of the "
+                "200M-event large axial FOV workload)",
+}
 UNIT = "LORs/s"
 
 
@@ -58,8 +66,10 @@ def parse_args(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
-    ap.add_argument("--workload", default="tor128", choices=["tor128", "batched96"],
-                    help="tor128: the headline TOF-TOR pair (default); batched96: 64-frame "
+    ap.add_argument("--workload", default="tor128", choices=["tor128", "large256", "batched96"],
+                    help="tor128: the headline TOF-TOR pair (default); large256: the same "
+                         "pair on one 16M-event chunk of the large axial FOV workload "
+                         "(256x256x128 at 2.5 mm, 1 m axial, 400 ps); batched96: 64-frame "
                          "batched OSEM iteration vs the plain per-frame loop")
     ap.add_argument("--frames", type=int, default=64)
     ap.add_argument("--tuning", default=None,
@@ -157,13 +167,17 @@ class ClockSampler:
 # --------------------------------------------------------------------- workload
 
 
-def workload_inputs(events_per_rank, rank, device):
+def workload_inputs(events_per_rank, rank, device, name="tor128"):
     from srf_b200 import synthetic as S
     from srf_b200.scanner import tof_info
-    wl = S.tor_128()
-    n = events_per_rank or wl.n_events
+    wl = S.large_256() if name == "large256" else S.tor_128()
+    chunk = 16_000_000 if name == "large256" else wl.n_events  # large FOV: streamed chunks
+    n = events_per_rank or chunk
     tof_bin, tof_sigma2 = tof_info(wl.tof_res_ps, wl.tof_bin_ps)
-    phantom = S.standard_phantom(half_length=wl.scanner.axial_length / 2)
+    if name == "large256":
+        phantom = S.large_fov_phantom(half_length=wl.scanner.axial_length / 2)
+    else:
+        phantom = S.standard_phantom(half_length=wl.scanner.axial_length / 2)
     events = S.generate_events(n, wl.scanner, phantom, seed=wl.seed + 7919 * rank,
                                tof_sigma_mm=math.sqrt(tof_sigma2), device=device)
     img = phantom.voxelize(wl.grid, wl.center, wl.size) + np.float32(0.05)
@@ -438,7 +452,8 @@ def main(argv=None):
     if args.tuning:
         from srf_b200 import tuning
         tuning.set_tuning(*[int(v) for v in args.tuning.split(",")])
-    wl, events, img_np, tof_bin, tof_sigma2 = workload_inputs(args.events, rank, dev)
+    wl, events, img_np, tof_bin, tof_sigma2 = workload_inputs(args.events, rank, dev,
+                                                              args.workload)
     n_events = events.shape[0]
     model = model_for(wl, tof_bin, tof_sigma2)
     groups = PP.recon_process(events, wl.tof_res_ps)
@@ -567,7 +582,7 @@ def main(argv=None):
                     "sample": f"unavailable: {exc}"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        line = {"metric": METRICS[args.workload], "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded events from a cylinder phantom)",
@@ -577,7 +592,8 @@ def main(argv=None):
                            "tof_bin_mm": tof_bin, "tof_sigma2": tof_sigma2,
                            "groups": {a: w["lors"] for a, w in work.items()},
                            "parallelism": f"events sharded, {world} rank(s)",
-                           "l2": "inputs larger than L2 (400 MB LOR records per rank)",
+                           "l2": "inputs larger than L2 (%d MB LOR records per rank)"
+                                 % (n_lors * 40 // 10**6),
                            "tuning": args.tuning or "automatic"},
                 "roofline": roof, "cpu_baseline": base, "e2e": e2e,
                 "gpu_launches": gpu_launches, "clocks": clk}

@@ -151,6 +151,12 @@ int srf_tor_backproject_adjoint_batched(const float *x1, const float *y1, const 
  * per slab, 0 = as many as fit; grid_mult: persistent slab CTAs = SMs x grid_mult (1..8). */
 int srf_tor_set_tuning(int path, int slab_slices, int grid_mult);
 
+/* No counterpart in the reference: upper bound, in bytes, of the per-slab LOR lists the
+ * slab kernels build per call (0 = the default, 1 GiB). The lists are sized for the worst
+ * case, 4 bytes x LORs x slabs per frame; a call with more LORs than fit is processed in
+ * chunks of LORs (at least 4096 each), each chunk a complete pass. Process-wide. */
+int srf_tor_set_scratch_limit(int64_t bytes);
+
 /* ---------------------------------------------------------------------------------- Siddon
  * Field columns for Siddon: x1,y1,z1,x2,y2,z2,tof (tof in mm along the LOR, the
  * reference's convention, siddon.cu.cc:460). Weight 1/L^2 (siddon.cu.cc:459). TOF on

@@ -542,6 +542,8 @@ constexpr int kSegTile = kSegThreads * kSegItems;
 constexpr int kMaxSlabs = 1024;
 constexpr int kSlabThreads = 1024;
 constexpr size_t kSlabSmemBytes = 220 * 1024;  // of the 227 KB a CTA can opt into
+// Budget of the per-slab LOR lists of one chunk of LORs (srf_tor_set_scratch_limit).
+std::atomic<long long> g_seg_scratch_bytes{1ll << 30};
 
 struct SegPlan {
     int nsl, n_slabs, ntiles;  // n_slabs counts slab ids over all frames
@@ -932,19 +934,37 @@ bool slab_geometry(const TorParams &p, int pad, int &nsl, int &n_slabs) {
     return (int64_t)n_slabs * std::max(1, p.n_frames) <= kMaxSlabs && p.n < (int64_t)INT32_MAX;
 }
 
+// Events [c0, c0 + n) of p as a call of their own (same images and outputs' layout).
+TorParams lor_chunk(const TorParams &p, int64_t c0, int64_t n) {
+    TorParams q = p;
+    const int64_t o = c0 * p.stride;
+    for (const float **c : {&q.x1, &q.y1, &q.z1, &q.x2, &q.y2, &q.z2, &q.xc, &q.yc, &q.zc, &q.f})
+        if (*c) *c += o;
+    if (q.values) q.values += c0;
+    if (q.proj_out) q.proj_out += c0;
+    if (q.frame) q.frame += c0;
+    q.n = n;
+    return q;
+}
+
 template <int OP, int P>
 int launch_slab(const TorParams &p, cudaStream_t stream) {
     SegPlan sp{};
     if (!slab_geometry(p, P - 1, sp.nsl, sp.slabs_pf)) return -1;
     sp.n_slabs = sp.slabs_pf * std::max(1, p.n_frames);
-    sp.ntiles = (int)((p.n + kSegTile - 1) / kSegTile);
-    // Scratch from the library's stream-ordered pool: no host synchronisation,
-    // capturable. The segment list is sized for the worst case (every LOR in every slab
-    // it can reach).
+    // The segment list is sized for the worst case (every LOR in every slab of its frame);
+    // LORs are taken in chunks small enough that this stays within the scratch budget
+    // (at least one 4096-LOR tile per chunk).
     const int64_t max_slabs_per_lor = sp.slabs_pf;
-    const size_t cap = (size_t)p.n * (size_t)max_slabs_per_lor;
+    const size_t budget = (size_t)g_seg_scratch_bytes.load(std::memory_order_relaxed);
+    int64_t chunk = (int64_t)(budget / (sizeof(int) * (size_t)max_slabs_per_lor));
+    chunk = std::max<int64_t>(kSegTile, chunk / kSegTile * kSegTile);
+    chunk = std::min<int64_t>(chunk, p.n);
+    sp.ntiles = (int)((chunk + kSegTile - 1) / kSegTile);
+    // Scratch from the library's stream-ordered pool: no host synchronisation, capturable.
+    const size_t cap = (size_t)chunk * (size_t)max_slabs_per_lor;
     auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
-    const size_t b_range = al(sizeof(int) * p.n);
+    const size_t b_range = al(sizeof(int) * chunk);
     const size_t b_counts = al(sizeof(int) * (size_t)sp.ntiles * sp.n_slabs);
     const size_t b_offs = al(sizeof(int64_t) * (size_t)sp.ntiles * sp.n_slabs);
     const size_t b_slab = al(sizeof(int64_t) * (2 * sp.n_slabs + 1));
@@ -988,14 +1008,20 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
             return SRF_ERR_CUDA;
         }
     }
-    seg_count_kernel<OP><<<sp.ntiles, kSegThreads, 0, stream>>>(p, sp);
-    seg_scan_kernel<<<sp.n_slabs, 1024, 0, stream>>>(sp, slab_tot);
-    seg_offsets_kernel<<<1, 32, 0, stream>>>(sp, slab_tot);
-    seg_fill_kernel<<<sp.ntiles, kSegThreads, 0, stream>>>(p, sp);
     const int mult = std::max(1, std::min(8, g_tune_mult.load(std::memory_order_relaxed)));
-    kern<<<num_sms() * mult, kSlabThreads, smem, stream>>>(p, sp);
-    count_launches(5);
-    int st = check_launch();
+    int st = SRF_OK;
+    for (int64_t c0 = 0; c0 < p.n && st == SRF_OK; c0 += chunk) {
+        const TorParams q = lor_chunk(p, c0, std::min(chunk, p.n - c0));
+        SegPlan sq = sp;
+        sq.ntiles = (int)((q.n + kSegTile - 1) / kSegTile);
+        seg_count_kernel<OP><<<sq.ntiles, kSegThreads, 0, stream>>>(q, sq);
+        seg_scan_kernel<<<sq.n_slabs, 1024, 0, stream>>>(sq, slab_tot);
+        seg_offsets_kernel<<<1, 32, 0, stream>>>(sq, slab_tot);
+        seg_fill_kernel<<<sq.ntiles, kSegThreads, 0, stream>>>(q, sq);
+        kern<<<num_sms() * mult, kSlabThreads, smem, stream>>>(q, sq);
+        count_launches(5);
+        st = check_launch();
+    }
     e = cudaFreeAsync(ws, stream);
     if (st == SRF_OK && e != cudaSuccess) {
         set_cuda_error(e);
@@ -1292,6 +1318,12 @@ extern "C" int srf_tor_backproject_adjoint_batched(
 // the autotuner. path: 0 automatic (slab kernels when a slice fits in shared memory),
 // 1 slab kernels, 2 LOR-centric kernels; slab_slices: slices per shared-memory slab
 // (0 = as many as fit); grid_mult: persistent slab CTAs = SMs x grid_mult (1..8).
+extern "C" int srf_tor_set_scratch_limit(int64_t bytes) {
+    if (bytes < 0) return SRF_ERR_INVALID_ARGUMENT;
+    g_seg_scratch_bytes.store(bytes == 0 ? (1ll << 30) : (long long)bytes);
+    return SRF_OK;
+}
+
 extern "C" int srf_tor_set_tuning(int path, int slab_slices, int grid_mult) {
     if (path < 0 || path > 3 || slab_slices < 0 || grid_mult < 1 || grid_mult > 8)
         return SRF_ERR_INVALID_ARGUMENT;

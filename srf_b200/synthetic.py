@@ -1,4 +1,4 @@
-"""Seeded synthetic list-mode workloads (the BASELINE configurations' shapes).
+"""Seeded synthetic list-mode workloads (the shapes of the benchmark configurations).
 
 No public dataset is involved: every event list is generated here from a fixed seed.
 
@@ -76,6 +76,20 @@ def standard_phantom(half_length=51.2, radius=100.0):
     return Phantom(radius=radius, half_length=half_length, activity=1.0, spheres=[
         Sphere((50.0, 0.0, 0.0), 5.0, 4.0), Sphere((-50.0, 0.0, 0.0), 5.0, 4.0),
         Sphere((0.0, 50.0, z), 5.0, 4.0), Sphere((0.0, -50.0, -z), 5.0, 4.0)])
+
+
+def large_fov_phantom(half_length=500.0, radius=200.0):
+    """Large axial FOV phantom: a cylinder r = 200 mm over the whole axial length with
+    eight spherical inserts along it, four hot (4:1, r = 20 mm) and four cold (activity
+    0, r = 25 mm), alternating around the axis."""
+    spheres = []
+    for k in range(8):
+        z = (k - 3.5) / 4.0 * half_length * 0.9
+        ph = k * math.pi / 4.0
+        hot = k % 2 == 0
+        spheres.append(Sphere((100.0 * math.cos(ph), 100.0 * math.sin(ph), z),
+                              20.0 if hot else 25.0, 4.0 if hot else 0.0))
+    return Phantom(radius=radius, half_length=half_length, activity=1.0, spheres=spheres)
 
 
 def random_phantom(seed, half_length, r_lo=60.0, r_hi=150.0):

@@ -28,6 +28,12 @@ def set_tuning(path=0, slab_slices=0, grid_mult=1):
     return (path, slab_slices, grid_mult)
 
 
+def set_scratch_limit(nbytes=0):
+    """Bound the per-call scratch of the slab kernels (``srf_tor_set_scratch_limit``);
+    larger calls run in chunks of LORs. 0 restores the default (1 GiB)."""
+    _lib.call("srf_tor_set_scratch_limit", int(nbytes))
+
+
 def candidates(max_slab_slices):
     """Settings worth trying: full and half-depth slabs, grid multipliers 1 and 2, the
     spread-items slab kernel and the LOR-centric kernels."""

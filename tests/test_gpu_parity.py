@@ -402,3 +402,37 @@ def test_tor_maplors_zero_divisor_matches_reference(scatter_kernel):
     fin = np.isfinite(ref)
     assert np.isnan(ref).any() and np.isinf(ref).any()
     assert K.rel_l2(gpu[fin], ref[fin]) <= TOL
+
+
+def test_slab_chunks_equal_one_pass():
+    """With the scratch budget forcing one 4096-LOR chunk at a time, every slab op gives
+    the single-pass result (projection values, images)."""
+    from srf_b200 import tuning
+    big = K.tor_case(n=40000, seed=91, grid=(128, 128, 64), voxel=3.2, n_box=4000)
+    kw, geo, b, s2 = _tp("tof530_kw10")
+    lors, img, g, c, s = K.tor_axis(big, "x")
+    assert lors.shape[1] > 3 * 4096
+    L, I = cu(lors), cu(img)
+    vals = cu(np.random.default_rng(3).random(lors.shape[1], dtype=np.float32) + 0.5)
+
+    def run():
+        pv = host(ops.tor_projection(L, I, g, c, s, kw, geo, b, s2, layout="cn"))
+        bp = host(ops.tor_backprojection(I, L, vals, g, c, s, kw, geo, b, s2, layout="cn"))
+        adj = host(ops.tor_backproject_adjoint(vals, L, g, c, s, kw, geo, b, s2, layout="cn"))
+        L7 = torch.cat([L[:6], L[9:10]]).contiguous()  # x1..z2, sigma2_factor
+        mp = host(ops.tor_maplors(I, g, c, s, L7, vals, kw, geo, layout="cn"))
+        return pv, bp, adj, mp
+
+    tuning.set_tuning(path=1)
+    try:
+        one = run()
+        tuning.set_scratch_limit(1)
+        try:
+            chunked = run()
+        finally:
+            tuning.set_scratch_limit(0)
+    finally:
+        tuning.set_tuning()
+    for a, b_ in zip(one, chunked):
+        assert np.count_nonzero(a) > 0
+        assert K.rel_l2(b_, a) <= 1e-6

@@ -1,6 +1,6 @@
 """The product kernels against the reference's OWN CUDA kernels (src/cpp/tf_custom_ops/
 tor.cu.cc and siddon.cu.cc built for sm_100a by oracle/Makefile), on the same B200 and
-the same inputs: the parity target of the north star (rel-L2 <= 1e-5 in float32).
+the same inputs: the parity target (rel-L2 <= 1e-5 in float32).
 
 Skipped where oracle/_ref was not built. Siddon inputs are first walked by the oracle:
 a ray whose first voxel falls off the grid would make the reference read outside the
