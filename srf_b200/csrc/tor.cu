@@ -332,27 +332,30 @@ __device__ __forceinline__ int trunc_div(float a, float b, float inv_b) {
 
 // One voxel slot: the reference's d^2 (tor.cu.cc:61-66, FMA-contracted as nvcc builds
 // it) and cut-off decision, and the folded exponent.
+// `cut` and `all` are the LOR's (L.cut, L.all) for a row the caller walks, -inf and false
+// for a row it must leave out (so the row costs no branch).
 template <int OP, typename F>
-__device__ __forceinline__ void slot(const LorConst &L, float dx, float dyuy, float dy2, float k0,
-                                     int ix, int iy, F &f) {
+__device__ __forceinline__ void slot(const LorConst &L, float cut, bool all, float dx, float dyuy,
+                                     float dy2, float k0, int ix, int iy, F &f) {
     const float rc = __fmaf_rn(dx, L.ux, dyuy);
     const float d2 = __fmaf_rn(-rc, rc, __fmaf_rn(dx, dx, dy2));
-    const bool in_cut = d2 < L.cut;
+    const bool in_cut = d2 < cut;
     const float e = fast_exp2(fmaf(d2, L.k1, k0));
     if (OP == kMap)
-        f(ix, iy, in_cut ? e : 0.0f, in_cut || L.all);
+        f(ix, iy, in_cut ? e : 0.0f, in_cut || all);
     else
         f(ix, iy, e, in_cut);
 }
 
 // W consecutive slots of one row.
 template <int OP, int W, int P, typename F>
-__device__ __forceinline__ void row_slots(const LorConst &L, const float (&dxs)[P], float dy,
-                                          float k0, int xlo, int iy, F &f) {
+__device__ __forceinline__ void row_slots(const LorConst &L, float cut, bool all,
+                                          const float (&dxs)[P], float dy, float k0, int xlo,
+                                          int iy, F &f) {
     const float dyuy = __fmul_rn(dy, L.uy);
     const float dy2 = __fmul_rn(dy, dy);
 #pragma unroll
-    for (int i = 0; i < W; i++) slot<OP>(L, dxs[i], dyuy, dy2, k0, xlo + i, iy, f);
+    for (int i = 0; i < W; i++) slot<OP>(L, cut, all, dxs[i], dyuy, dy2, k0, xlo + i, iy, f);
 }
 
 // g(std::integral_constant<int, w>{}) for a runtime width 1 <= w <= P.
@@ -374,13 +377,16 @@ __device__ __forceinline__ void with_width(int w, G &&g) {
 // w = 0 outside the cut-off, as the reference adds 0/0 there). Returns the number of
 // in-slice window voxels (for kCount).
 //
-// kPadded: the caller's slice has P - 1 zero rows and columns around the grid (the
-// shared-memory slab), so window voxels outside the grid need no test: a gather reads 0
-// there and a scatter lands in padding that is never flushed. The walked box is then
-// widened to the warp's largest (kept inside the window), which makes the trip counts
-// warp-uniform. Otherwise the box is clipped to the grid.
-template <int OP, int P, bool kPadded, typename F>
-__device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L, int s, F &&f) {
+// Only rows R0 <= iy < R1 are walked (a band of rows of the grid, or all of it).
+// kPadded: the caller's slice has P - 1 zero columns on both sides of the grid and P - 1
+// spare rows above and below the band (the shared-memory slab), so window columns
+// outside the grid need no test: a gather reads 0 there and a scatter lands in padding
+// that is never flushed. The walked box is then widened to the warp's largest (kept
+// inside the window), which makes the trip counts warp-uniform; rows the widening adds
+// outside the band are masked. Otherwise the box is clipped to the grid.
+template <int OP, int P, bool kPadded, bool kBand, typename F>
+__device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L, int s, int R0,
+                                           int R1, F &&f) {
     const float sz = slice_z<OP>(p, s);
     const float ratio = __fdiv_rn(__fsub_rn(sz, L.z1), L.dz);
     if (!(ratio > 0.0f && ratio < 1.0f)) return 0;
@@ -402,11 +408,15 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
     int xhi = min(ix0 + P - 1, __float2int_rd(fx + L.bxv));
     int ylo = max(iy0, __float2int_ru(fy - L.byv));
     int yhi = min(iy0 + P - 1, __float2int_rd(fy + L.byv));
+    // A slab holding whole slices has zero padding rows too; only a band needs row limits.
+    constexpr bool banded = !kPadded || kBand;
+    if (banded) {
+        ylo = max(ylo, R0);
+        yhi = min(yhi, R1 - 1);
+    }
     if (!kPadded) {
         xlo = max(xlo, 0);
         xhi = min(xhi, p.gx - 1);
-        ylo = max(ylo, 0);
-        yhi = min(yhi, p.gy - 1);
     }
     int wx = xhi - xlo + 1, wy = yhi - ylo + 1;
     if (wx <= 0 || wy <= 0) return n_slots;
@@ -436,23 +446,47 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
         // loads issue back to back. The gather picks the body once per slice; the scatter
         // (a compare-and-swap loop per voxel in shared memory) runs faster picking it per
         // row (measured).
+        // In a band, rows the widening added outside [R0, R1) (another band's, or off
+        // the grid) are masked through their cut-off; the walked rows stay within the
+        // slab's padding rows. Whole slices need no mask (their padding rows read 0).
         const float fy0 = (float)ylo + 0.5f;
-        if (OP == kProj) {
-            with_width<P>(wx, [&](auto W) {
+        auto walk = [&](auto masked) {
+            constexpr bool kMask = decltype(masked)::value;
+            auto row_cut = [&](int j, bool &all) {
+                if constexpr (kMask) {
+                    const bool in_band = (unsigned)(ylo + j - R0) < (unsigned)(R1 - R0);
+                    all = in_band && L.all;
+                    return in_band ? L.cut : -INFINITY;
+                } else {
+                    all = L.all;
+                    return L.cut;
+                }
+            };
+            if (OP == kProj) {
+                with_width<P>(wx, [&](auto W) {
+                    for (int j = 0; j < wy; j++) {
+                        bool all;
+                        const float cut = row_cut(j, all);
+                        const float dy =
+                            __fsub_rn(cy, __fmaf_rn(p.inter_y, fy0 + (float)j, p.b_bound));
+                        row_slots<OP, decltype(W)::value>(L, cut, all, dxs, dy, k0, xlo, ylo + j,
+                                                          f);
+                    }
+                });
+            } else {
                 for (int j = 0; j < wy; j++) {
+                    bool all;
+                    const float cut = row_cut(j, all);
                     const float dy =
                         __fsub_rn(cy, __fmaf_rn(p.inter_y, fy0 + (float)j, p.b_bound));
-                    row_slots<OP, decltype(W)::value>(L, dxs, dy, k0, xlo, ylo + j, f);
+                    with_width<P>(wx, [&](auto W) {
+                        row_slots<OP, decltype(W)::value>(L, cut, all, dxs, dy, k0, xlo, ylo + j,
+                                                          f);
+                    });
                 }
-            });
-        } else {
-            for (int j = 0; j < wy; j++) {
-                const float dy = __fsub_rn(cy, __fmaf_rn(p.inter_y, fy0 + (float)j, p.b_bound));
-                with_width<P>(wx, [&](auto W) {
-                    row_slots<OP, decltype(W)::value>(L, dxs, dy, k0, xlo, ylo + j, f);
-                });
             }
-        }
+        };
+        walk(std::integral_constant<bool, kBand>{});
     } else {
 #pragma unroll
         for (int j = 0; j < P; j++) {
@@ -464,7 +498,7 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
 #pragma unroll
             for (int i = 0; i < P; i++) {
                 if (i >= wx) break;
-                slot<OP>(L, dxs[i], dyuy, dy2, k0, xlo + i, iy, f);
+                slot<OP>(L, L.cut, L.all, dxs[i], dyuy, dy2, k0, xlo + i, iy, f);
             }
         }
     }
@@ -488,7 +522,7 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
             const int64_t img0 = frame_offset(p, t);
             for (int s = L.s_lo + lane; s <= L.s_hi; s += 32) {
                 const int64_t base = img0 + (int64_t)s * slice_mesh;
-                n_slots += slice_visit<OP, P, false>(p, L, s,
+                n_slots += slice_visit<OP, P, false, false>(p, L, s, 0, p.gy,
                                                      [&](int ix, int iy, float w, bool use) {
                     const int64_t idx = base + (int64_t)iy * p.gx + ix;
                     if (OP == kCount) {
@@ -539,7 +573,7 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
 constexpr int kSegThreads = 512;
 constexpr int kSegItems = 8;
 constexpr int kSegTile = kSegThreads * kSegItems;
-constexpr int kMaxSlabs = 1024;
+constexpr int kMaxSlabs = 4096;
 constexpr int kSlabThreads = 1024;
 constexpr size_t kSlabSmemBytes = 220 * 1024;  // of the 227 KB a CTA can opt into
 // Budget of the per-slab LOR lists of one chunk of LORs (srf_tor_set_scratch_limit).
@@ -547,7 +581,8 @@ std::atomic<long long> g_seg_scratch_bytes{1ll << 30};
 
 struct SegPlan {
     int nsl, n_slabs, ntiles;  // n_slabs counts slab ids over all frames
-    int slabs_pf;              // slabs per frame
+    int slabs_pf;              // slice ranges per frame
+    int nbands, band_rows;     // row bands per slice range and rows per band (last: fewer)
     int *range;            // [n] packed k_lo | k_hi << 16, or -1
     int *tile_counts;      // [ntiles * n_slabs]
     int64_t *tile_offs;    // [ntiles * n_slabs]
@@ -555,9 +590,48 @@ struct SegPlan {
     int *seg;              // [capacity] LOR indices, slab-major
 };
 
-template <int OP>
+// Slab ids of LOR t (slice range k of its frame, row band b): id = k * nbands + b, with k
+// counted over frames. Calls g(id) for each. With row bands, the bands of slice range k
+// are those the LOR's window rows can reach in its slices there: the rows follow the
+// crossing point's y, which is monotonic in the slice, so the rows of the range's two end
+// slices, with two rows of margin and the window's extent, bound them.
+template <bool kBand, typename G>
+__device__ __forceinline__ void lor_slab_ids(const TorParams &p, const SegPlan &sp, int64_t t,
+                                             int k_lo, int k_hi, int s_lo, int s_hi, G &&g) {
+    if constexpr (!kBand) {
+        for (int k = k_lo; k <= k_hi; k++) g(k);
+        return;
+    }
+    const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
+    const int64_t o = t * p.stride;
+    const float y1 = __ldg(p.y1 + o), y2 = __ldg(p.y2 + o);
+    const float z1 = __ldg(p.z1 + o), z2 = __ldg(p.z2 + o);
+    auto y_at = [&](int s) {
+        const float r = (p.slice0_f + (float)s * p.inter_z - z1) / (z2 - z1);
+        return fmaf(y2 - y1, fminf(fmaxf(r, 0.0f), 1.0f), y1);
+    };
+    for (int k = k_lo; k <= k_hi; k++) {
+        const int first = (k - f0) * sp.nsl;
+        const float ya = y_at(max(s_lo, first)), yb = y_at(min(s_hi, first + sp.nsl - 1));
+        const float lo = fminf(ya, yb), hi = fmaxf(ya, yb);
+        int b_lo = 0, b_hi = sp.nbands - 1;
+        if (lo == lo && hi == hi) {  // else: every band, left to the exact per-slice test
+            const float flo = fminf(fmaxf(floorf((lo - p.b_bound) * p.inv_y), -1.0e8f), 1.0e8f);
+            const float fhi = fminf(fmaxf(floorf((hi - p.b_bound) * p.inv_y), -1.0e8f), 1.0e8f);
+            const int r_lo = max((int)flo - p.half - 2, 0);
+            const int r_hi = min((int)fhi - p.half + p.patch + 1, p.gy - 1);
+            if (r_lo > r_hi) continue;
+            b_lo = r_lo / sp.band_rows;
+            b_hi = min(r_hi / sp.band_rows, sp.nbands - 1);
+        }
+        for (int b = b_lo; b <= b_hi; b++) g(k * sp.nbands + b);
+    }
+}
+
+// kBand: sp.nbands > 1 (slab ids over slice ranges and row bands).
+template <int OP, bool kBand>
 __global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams p, SegPlan sp) {
-    __shared__ int hist[kMaxSlabs];
+    extern __shared__ int hist[];  // [n_slabs]
     for (int k = threadIdx.x; k < sp.n_slabs; k += kSegThreads) hist[k] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kSegTile;
@@ -571,7 +645,8 @@ __global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams 
             const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
             const int k_lo = f0 + s_lo / sp.nsl, k_hi = f0 + s_hi / sp.nsl;
             packed = k_lo | (k_hi << 16);
-            for (int k = k_lo; k <= k_hi; k++) atomicAdd(&hist[k], 1);
+            lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi,
+                                [&](int id) { atomicAdd(&hist[id], 1); });
         }
         sp.range[t] = packed;
     }
@@ -628,8 +703,9 @@ __global__ void seg_offsets_kernel(SegPlan sp, const int64_t *slab_tot) {
     }
 }
 
+template <bool kBand>
 __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p, SegPlan sp) {
-    __shared__ int cursor[kMaxSlabs];
+    extern __shared__ int cursor[];  // [n_slabs]
     for (int k = threadIdx.x; k < sp.n_slabs; k += kSegThreads) cursor[k] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kSegTile;
@@ -639,11 +715,13 @@ __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p
         const int packed = sp.range[t];
         if (packed < 0) continue;
         const int k_lo = packed & 0xffff, k_hi = packed >> 16;
-        for (int k = k_lo; k <= k_hi; k++) {
-            const int pos = atomicAdd(&cursor[k], 1);
-            sp.seg[sp.slab_offs[k] + sp.tile_offs[(int64_t)blockIdx.x * sp.n_slabs + k] + pos] =
+        int s_lo = 0, s_hi = p.gz - 1;
+        if (kBand) lor_slices(p, t, s_lo, s_hi);  // same range as seg_count's
+        lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi, [&](int id) {
+            const int pos = atomicAdd(&cursor[id], 1);
+            sp.seg[sp.slab_offs[id] + sp.tile_offs[(int64_t)blockIdx.x * sp.n_slabs + id] + pos] =
                 (int)t;
-        }
+        });
     }
 }
 
@@ -703,7 +781,8 @@ __host__ __device__ __forceinline__ int slab_floats(int nsl, int gx, int gy, int
 // kExpand: the (LOR, slice) items of a warp's 32 segments are spread over its lanes, 32
 // at a time (one item per lane, LOR constants shuffled to it); otherwise each lane walks
 // its own segment's slices.
-template <int OP, int P, bool kExpand>
+// kBand: the slabs are bands of rows (sp.nbands > 1), so rows are limited to the band.
+template <int OP, int P, bool kExpand, bool kBand>
 __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorParams p, SegPlan sp) {
     extern __shared__ float slab[];
     __shared__ signed char owner_tab[kSlabThreads / 32][32];
@@ -711,15 +790,15 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
     constexpr int kWarps = kSlabThreads / 32;
     const int slice_mesh = p.gx * p.gy;
     constexpr int pad = P - 1;
-    const int rs = slab_row_stride(p.gx, pad), ss = slab_slice_stride(p.gx, p.gy, pad);
+    const int rs = slab_row_stride(p.gx, pad), ss = slab_slice_stride(p.gx, sp.band_rows, pad);
     const int origin = slab_origin(p.gx, pad);
     const int64_t total = sp.slab_offs[sp.n_slabs];
     const int64_t g = blockIdx.x, G = gridDim.x;
     const int64_t lo = total * g / G, hi = total * (g + 1) / G;
     if (lo >= hi) return;
     if (OP == kProj) {
-        // The padding stays zero: the slab loads below write grid voxels only.
-        const int n = slab_floats(sp.nsl, p.gx, p.gy, pad);
+        // The padding columns stay zero: the slab loads below write grid voxels only.
+        const int n = slab_floats(sp.nsl, p.gx, sp.band_rows, pad);
         for (int i = threadIdx.x; i < n; i += kSlabThreads) slab[i] = 0.0f;
         __syncthreads();
     }
@@ -736,21 +815,25 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
     while (pos < hi) {
         while (sp.slab_offs[k + 1] <= pos) k++;  // skip empty slabs
         const int64_t end = min(hi, sp.slab_offs[k + 1]);
-        const int fr = k / sp.slabs_pf;
-        const int S0 = (k - fr * sp.slabs_pf) * sp.nsl;
+        // slab id -> frame, slice range, row band
+        const int per_frame = sp.slabs_pf * sp.nbands;
+        const int fr = k / per_frame;
+        const int kk = (k - fr * per_frame) / sp.nbands, band = k - fr * per_frame - kk * sp.nbands;
+        const int S0 = kk * sp.nsl, S1 = min(S0 + sp.nsl, p.gz);
+        const int R0 = band * sp.band_rows, R1 = min(R0 + sp.band_rows, p.gy);
+        const int nbr = R1 - R0;
         const int64_t img0 = (int64_t)fr * p.frame_stride;
-        const int S1 = min(S0 + sp.nsl, p.gz);
-        const int n_rows = (S1 - S0) * p.gy;
+        const int n_rows = (S1 - S0) * nbr;
         if (OP == kProj) {
-            const float *src = p.image_in + img0 + (int64_t)S0 * slice_mesh;
+            const float *src = p.image_in + img0 + (int64_t)S0 * slice_mesh + (int64_t)R0 * p.gx;
             for (int r = warp; r < n_rows; r += kWarps) {
-                const int sl = r / p.gy, iy = r - sl * p.gy;
-                const float *g = src + (int64_t)r * p.gx;
+                const int sl = r / nbr, iy = r - sl * nbr;
+                const float *g = src + (int64_t)sl * slice_mesh + (int64_t)iy * p.gx;
                 float *d = slab + origin + sl * ss + iy * rs;
                 for (int ix = lane; ix < p.gx; ix += 32) d[ix] = __ldg(g + ix);
             }
         } else {
-            const int n = slab_floats(S1 - S0, p.gx, p.gy, pad);
+            const int n = slab_floats(S1 - S0, p.gx, sp.band_rows, pad);
             for (int i = threadIdx.x; i < n; i += kSlabThreads) slab[i] = 0.0f;
         }
         __syncthreads();
@@ -769,15 +852,17 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                 float acc = 0.0f;
                 for (int i = 0; i < cnt; i++) {
                     const int s = a + i;
-                    float *sb = slab + origin + (s - S0) * ss;
+                    float *sb = slab + origin + (s - S0) * ss;  // slice s, row R0
                     if (OP == kProj) {
-                        slice_visit<OP, P, true>(p, L, s, [&](int ix, int iy, float w, bool use) {
-                            const float v = sb[iy * rs + ix];
+                        slice_visit<OP, P, true, kBand>(p, L, s, R0, R1,
+                                                 [&](int ix, int iy, float w, bool use) {
+                            const float v = sb[(iy - R0) * rs + ix];
                             acc = use ? fmaf(w, v, acc) : acc;
                         });
                     } else {
-                        slice_visit<OP, P, true>(p, L, s, [&](int ix, int iy, float w, bool use) {
-                            if (use) atomicAdd(&sb[iy * rs + ix], w * L.scale);
+                        slice_visit<OP, P, true, kBand>(p, L, s, R0, R1,
+                                                 [&](int ix, int iy, float w, bool use) {
+                            if (use) atomicAdd(&sb[(iy - R0) * rs + ix], w * L.scale);
                         });
                     }
                 }
@@ -807,17 +892,19 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                 float partial = 0.0f;
                 if (valid) {
                     const int s = a_o + (item - excl_o);
-                    float *sb = slab + origin + (s - S0) * ss;
+                    float *sb = slab + origin + (s - S0) * ss;  // slice s, row R0
                     if (OP == kProj) {
                         float acc = 0.0f;
-                        slice_visit<OP, P, true>(p, M, s, [&](int ix, int iy, float w, bool use) {
-                            const float v = sb[iy * rs + ix];
+                        slice_visit<OP, P, true, kBand>(p, M, s, R0, R1,
+                                                 [&](int ix, int iy, float w, bool use) {
+                            const float v = sb[(iy - R0) * rs + ix];
                             acc = use ? fmaf(w, v, acc) : acc;
                         });
                         partial = acc * M.scale;
                     } else {
-                        slice_visit<OP, P, true>(p, M, s, [&](int ix, int iy, float w, bool use) {
-                            if (use) atomicAdd(&sb[iy * rs + ix], w * M.scale);
+                        slice_visit<OP, P, true, kBand>(p, M, s, R0, R1,
+                                                 [&](int ix, int iy, float w, bool use) {
+                            if (use) atomicAdd(&sb[(iy - R0) * rs + ix], w * M.scale);
                         });
                     }
                 }
@@ -838,11 +925,11 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
         }
         __syncthreads();
         if (OP != kProj) {
-            float *out = p.image_out + img0 + (int64_t)S0 * slice_mesh;
+            float *out = p.image_out + img0 + (int64_t)S0 * slice_mesh + (int64_t)R0 * p.gx;
             for (int r = warp; r < n_rows; r += kWarps) {
-                const int sl = r / p.gy, iy = r - sl * p.gy;
+                const int sl = r / nbr, iy = r - sl * nbr;
                 const float *src = slab + origin + sl * ss + iy * rs;
-                float *g = out + (int64_t)r * p.gx;
+                float *g = out + (int64_t)sl * slice_mesh + (int64_t)iy * p.gx;
                 for (int ix = lane; ix < p.gx; ix += 32) {
                     const float v = src[ix];
                     if (v != 0.0f) atomicAdd(g + ix, v);
@@ -919,19 +1006,45 @@ void launch_p(const TorParams &p, int grid, int block, cudaStream_t stream) {
     count_launches(1);
 }
 
-// Slices per slab (as many as fit in shared memory) and slab count; false when one
-// slice does not fit (the global-atomics kernel is used then).
-bool slab_geometry(const TorParams &p, int pad, int &nsl, int &n_slabs) {
+// Slab shape: slices per slab, slice ranges per frame, row bands and rows per band.
+// Whole slices when at least kMinSlabSlices of them fit in shared memory (or the tuned
+// count fits); otherwise bands of rows, as tall as fit for that many slices (fewer
+// slices if not even kMinBandRows rows fit). False when nothing fits or there are too
+// many slab ids (the LOR-centric kernels are used then).
+constexpr int kMinSlabSlices = 4;
+constexpr int kMinBandRows = 8;
+
+bool slab_geometry(const TorParams &p, int pad, SegPlan &sp) {
     if (p.gx > (1 << 14) || p.gy > (1 << 14)) return false;
-    const size_t slice_floats = (size_t)slab_slice_stride(p.gx, p.gy, pad);
-    const size_t fixed = (size_t)slab_origin(p.gx, pad);
     const size_t budget = kSlabSmemBytes / sizeof(float);
-    if (slice_floats + fixed > budget) return false;
-    nsl = (int)std::min<size_t>((budget - fixed) / slice_floats, (size_t)p.gz);
+    auto fits = [&](int n, int rows) {
+        return (size_t)slab_floats(n, p.gx, rows, pad) <= budget;
+    };
+    int full = 0;
+    while (full < p.gz && fits(full + 1, p.gy)) full++;
     const int want = g_tune_nsl.load(std::memory_order_relaxed);
-    if (want > 0) nsl = std::min(nsl, want);
-    n_slabs = (p.gz + nsl - 1) / nsl;
-    return (int64_t)n_slabs * std::max(1, p.n_frames) <= kMaxSlabs && p.n < (int64_t)INT32_MAX;
+    if ((want == 0 && full >= std::min(kMinSlabSlices, p.gz)) || (want > 0 && want <= full)) {
+        sp.nsl = want > 0 ? want : full;
+        sp.band_rows = p.gy;
+    } else {
+        int n = std::min(want > 0 ? want : kMinSlabSlices, p.gz);
+        sp.band_rows = 0;
+        for (; n >= 1; n--) {
+            int rows = std::min(p.gy, (int)((budget / n) / (size_t)slab_row_stride(p.gx, pad)));
+            while (rows > 0 && !fits(n, rows)) rows--;
+            if (rows >= std::min(p.gy, kMinBandRows)) {
+                sp.band_rows = rows;
+                break;
+            }
+        }
+        if (sp.band_rows == 0) return false;
+        sp.nsl = n;
+    }
+    sp.nbands = (p.gy + sp.band_rows - 1) / sp.band_rows;
+    sp.slabs_pf = (p.gz + sp.nsl - 1) / sp.nsl;
+    sp.n_slabs = sp.slabs_pf * sp.nbands * std::max(1, p.n_frames);
+    return sp.n_slabs <= kMaxSlabs && sp.slabs_pf * std::max(1, p.n_frames) < (1 << 16) &&
+           p.n < (int64_t)INT32_MAX;
 }
 
 // Events [c0, c0 + n) of p as a call of their own (same images and outputs' layout).
@@ -950,12 +1063,11 @@ TorParams lor_chunk(const TorParams &p, int64_t c0, int64_t n) {
 template <int OP, int P>
 int launch_slab(const TorParams &p, cudaStream_t stream) {
     SegPlan sp{};
-    if (!slab_geometry(p, P - 1, sp.nsl, sp.slabs_pf)) return -1;
-    sp.n_slabs = sp.slabs_pf * std::max(1, p.n_frames);
+    if (!slab_geometry(p, P - 1, sp)) return -1;
     // The segment list is sized for the worst case (every LOR in every slab of its frame);
     // LORs are taken in chunks small enough that this stays within the scratch budget
     // (at least one 4096-LOR tile per chunk).
-    const int64_t max_slabs_per_lor = sp.slabs_pf;
+    const int64_t max_slabs_per_lor = (int64_t)sp.slabs_pf * sp.nbands;
     const size_t budget = (size_t)g_seg_scratch_bytes.load(std::memory_order_relaxed);
     int64_t chunk = (int64_t)(budget / (sizeof(int) * (size_t)max_slabs_per_lor));
     chunk = std::max<int64_t>(kSegTile, chunk / kSegTile * kSegTile);
@@ -982,10 +1094,12 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
     sp.slab_offs = reinterpret_cast<int64_t *>(ws + b_range + b_counts + b_offs);
     sp.seg = reinterpret_cast<int *>(ws + b_range + b_counts + b_offs + b_slab);
 
+    const bool band = sp.nbands > 1;
     void (*kern)(const TorParams, SegPlan) =
-        p.slab_expand ? tor_slab_kernel<OP, P, true> : tor_slab_kernel<OP, P, false>;
-    static std::atomic<unsigned long long> attr_set[2];  // per kernel instance, per device
-    std::atomic<unsigned long long> &done = attr_set[p.slab_expand ? 1 : 0];
+        p.slab_expand ? (band ? tor_slab_kernel<OP, P, true, true> : tor_slab_kernel<OP, P, true, false>)
+                      : (band ? tor_slab_kernel<OP, P, false, true> : tor_slab_kernel<OP, P, false, false>);
+    static std::atomic<unsigned long long> attr_set[4];  // per kernel instance, per device
+    std::atomic<unsigned long long> &done = attr_set[(p.slab_expand ? 2 : 0) + (band ? 1 : 0)];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
     if (!(done.load() & (1ull << dev))) {
@@ -998,7 +1112,7 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
         }
         done.fetch_or(1ull << dev);
     }
-    const size_t smem = sizeof(float) * (size_t)slab_floats(sp.nsl, p.gx, p.gy, P - 1);
+    const size_t smem = sizeof(float) * (size_t)slab_floats(sp.nsl, p.gx, sp.band_rows, P - 1);
     int64_t *slab_tot = sp.slab_offs + sp.n_slabs + 1;
     if (OP == kProj) {
         e = cudaMemsetAsync(p.proj_out, 0, sizeof(float) * p.n, stream);
@@ -1009,15 +1123,22 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
         }
     }
     const int mult = std::max(1, std::min(8, g_tune_mult.load(std::memory_order_relaxed)));
+    const size_t hist_bytes = sizeof(int) * (size_t)sp.n_slabs;  // <= 16 KB (kMaxSlabs)
     int st = SRF_OK;
     for (int64_t c0 = 0; c0 < p.n && st == SRF_OK; c0 += chunk) {
         const TorParams q = lor_chunk(p, c0, std::min(chunk, p.n - c0));
         SegPlan sq = sp;
         sq.ntiles = (int)((q.n + kSegTile - 1) / kSegTile);
-        seg_count_kernel<OP><<<sq.ntiles, kSegThreads, 0, stream>>>(q, sq);
+        if (band)
+            seg_count_kernel<OP, true><<<sq.ntiles, kSegThreads, hist_bytes, stream>>>(q, sq);
+        else
+            seg_count_kernel<OP, false><<<sq.ntiles, kSegThreads, hist_bytes, stream>>>(q, sq);
         seg_scan_kernel<<<sq.n_slabs, 1024, 0, stream>>>(sq, slab_tot);
         seg_offsets_kernel<<<1, 32, 0, stream>>>(sq, slab_tot);
-        seg_fill_kernel<<<sq.ntiles, kSegThreads, 0, stream>>>(q, sq);
+        if (band)
+            seg_fill_kernel<true><<<sq.ntiles, kSegThreads, hist_bytes, stream>>>(q, sq);
+        else
+            seg_fill_kernel<false><<<sq.ntiles, kSegThreads, hist_bytes, stream>>>(q, sq);
         kern<<<num_sms() * mult, kSlabThreads, smem, stream>>>(q, sq);
         count_launches(5);
         st = check_launch();

@@ -69,18 +69,19 @@ def tcase():
     return K.tor_case(n=3000, seed=31, grid=(128, 128, 64), voxel=3.2, n_box=600)
 
 
-# Tuning paths of the TOR kernels: shared-memory slabs with a lane per (LOR, slab)
-# segment (1, the default), slabs with a segment's slices spread over lanes (3), and
+# Tuning of the TOR kernels, (path, slices per slab): shared-memory slabs with a lane per
+# (LOR, slab) segment (1, the default), the same with 16 slices per slab, which splits
+# every slice into bands of rows, slabs with a segment's slices spread over lanes (3), and
 # LOR-centric kernels reading the image from L2 with global atomics (2, the fallback when
-# a slice does not fit in shared memory).
-TOR_PATHS = {"slab": 1, "slab_spread": 3, "global": 2}
+# nothing fits in shared memory).
+TOR_PATHS = {"slab": (1, 0), "slab_bands": (1, 16), "slab_spread": (3, 0), "global": (2, 0)}
 
 
 @pytest.fixture(params=list(TOR_PATHS))
 def tor_path(request):
     """Every TOR kernel family must agree with the oracle."""
     from srf_b200 import tuning
-    tuning.set_tuning(path=TOR_PATHS[request.param])
+    tuning.set_tuning(*TOR_PATHS[request.param])
     yield request.param
     tuning.set_tuning()
 
@@ -109,7 +110,7 @@ def test_tor_projection(tcase, pname, axis, tor_path):
 def scatter_kernel(request):
     """Back-projection / map / adjoint in every TOR kernel family against the oracle."""
     from srf_b200 import tuning
-    tuning.set_tuning(path=TOR_PATHS[request.param])
+    tuning.set_tuning(*TOR_PATHS[request.param])
     yield request.param
     tuning.set_tuning()
 

@@ -144,10 +144,12 @@ def _frames(n_frames, seed, grid=(48, 48, 24), voxel=6.4):
     return frames, list(grid), size
 
 
-@pytest.mark.parametrize("path", [1, 2, 3])
-def test_batched_ops_equal_per_frame(path):
+@pytest.mark.parametrize("tune", [(1, 0), (1, 16), (2, 0), (3, 0)])
+def test_batched_ops_equal_per_frame(tune):
+    """Batched ops equal per-frame calls in every kernel family (slab ids run over
+    frames x slice ranges x row bands; (1, 16) forces row bands)."""
     from srf_b200 import tuning
-    tuning.set_tuning(path=path)
+    tuning.set_tuning(*tune)
     try:
         frames, grid, size = _frames(5, 1)
         b, s2 = K.tof_params(530.0)

@@ -34,7 +34,7 @@ def tcase():
 @pytest.fixture(params=list(TOR_PATHS))
 def tor_path(request):
     from srf_b200 import tuning
-    tuning.set_tuning(path=TOR_PATHS[request.param])
+    tuning.set_tuning(*TOR_PATHS[request.param])
     yield request.param
     tuning.set_tuning()
 
