@@ -52,6 +52,7 @@ METRICS = {
     "tor128": METRIC,
     "large256": "TOF-TOR proj+backproj LORs/s at 256x256x128 (16M-event chunk of the "
                 "200M-event large axial FOV workload)",
+    "siddon64": "non-TOF Siddon proj+backproj LORs/s at 64x64x32 (1M events)",
 }
 UNIT = "LORs/s"
 
@@ -66,10 +67,13 @@ def parse_args(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
-    ap.add_argument("--workload", default="tor128", choices=["tor128", "large256", "batched96"],
+    ap.add_argument("--workload", default="tor128",
+                    choices=["tor128", "large256", "siddon64", "batched96"],
                     help="tor128: the headline TOF-TOR pair (default); large256: the same "
                          "pair on one 16M-event chunk of the large axial FOV workload "
-                         "(256x256x128 at 2.5 mm, 1 m axial, 400 ps); batched96: 64-frame "
+                         "(256x256x128 at 2.5 mm, 1 m axial, 400 ps); siddon64: the plain "
+                         "non-TOF Siddon pair and OSEM iteration (64x64x32, 1M events); "
+                         "batched96: 64-frame "
                          "batched OSEM iteration vs the plain per-frame loop")
     ap.add_argument("--frames", type=int, default=64)
     ap.add_argument("--tuning", default=None,
@@ -278,6 +282,192 @@ def cpu_baseline(groups_host, wl, tof_bin, tof_sigma2, image_np, target_s):
                       f"{t1:.1f} s wall"}
 
 
+def run_siddon(args):
+    """Plain non-TOF Siddon (the CPU-runnable configuration): R 400 mm, 400 x 32
+    crystals, 64x64x32 image at 3.4 mm, 1M seeded events from the cylinder phantom,
+    tof_sigma2 = 1e6 (at or above the reference's TOF switch, so TOF is off). One step =
+    Siddon projection of all events, then the reference back-projection A^T(1/Ax). Also
+    times one OSEM iteration (4 subsets, effmap from 10M random crystal pairs) and the
+    reference's host-built Siddon pair on a bounded sample."""
+    from srf_b200 import CompleteLoRsModel, Image, backprojection, ops, profiling, projection
+    from srf_b200 import recon
+    from srf_b200 import synthetic as S
+    from srf_b200 import _lib
+    from srf_b200.data import ListModeData
+    from srf_b200.preprocess import initial_image
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    wl = S.siddon_64()
+    n = args.events or wl.n_events
+    phantom = S.standard_phantom(half_length=wl.scanner.axial_length / 2)
+    events = S.generate_events(n, wl.scanner, phantom, seed=wl.seed + 7919 * rank, device=dev)
+    img_np = phantom.voxelize(wl.grid, wl.center, wl.size) + np.float32(0.05)
+    image = Image(torch.as_tensor(img_np, device=dev), wl.center, wl.size)
+    model = CompleteLoRsModel(tof_sigma2=1.0e6, tof_bin=1.0e4)
+    data = ListModeData(events, torch.ones(events.shape[0], device=dev))
+    kimg, g, c, sz = model.kernel_geometry(image)
+    visits = int(ops.siddon_count_samples(events, g, c, sz, layout="nc").sum(dtype=torch.int64))
+
+    def step():
+        p = projection(model, image, data)
+        bp = backprojection(model, p, image)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(bp.data)
+        return bp
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    timer = profiling.KernelTimer()
+    launches0 = _lib.call_raw("srf_launch_count")
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with timer:
+        start.record()
+        for _ in range(args.steps):
+            step()
+        end.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    gpu_launches = _lib.call_raw("srf_launch_count") - launches0
+    ms = max_over_ranks(start.elapsed_time(end), world)
+    clk = clocks.stop() if clocks else None
+    kern = timer.summary()
+    value = n * world * args.steps / (ms / 1e3)
+
+    # e2e through the public API from pinned host events
+    e2e = None
+    if args.e2e_steps > 0:
+        host_events = events.cpu().pin_memory()
+
+        def e2e_step():
+            ev = host_events.to(dev, non_blocking=True)
+            d = ListModeData(ev, torch.ones(ev.shape[0], device=dev))
+            bp = backprojection(model, projection(model, image, d), image)
+            return bp.data.cpu()
+
+        e2e_step()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        s1.record()
+        torch.cuda.synchronize()
+        e_ms = max_over_ranks(s0.elapsed_time(s1), world)
+        e2e = {"value": n * world * args.e2e_steps / (e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": host_events.numel() * 4,
+               "d2h_bytes_per_step": int(np.prod(wl.grid)) * 4,
+               "ms_per_step": e_ms / args.e2e_steps,
+               "path": "pinned host events -> projection -> backprojection -> host image"}
+
+    # one OSEM iteration (4 subsets) with the effmap of 10M random crystal pairs
+    lors = S.random_lors(10_000_000, wl.scanner, 77, device=dev)
+    effinv, _ = recon.efficiency_map(model, lors, list(wl.grid), wl.center, wl.size,
+                                     wl.scanner.inner_radius, wl.scanner.axial_length)
+    del lors
+    x0 = initial_image(list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
+                       wl.scanner.axial_length, dev)
+    osem = recon.OSEM(model, data, effinv, Image(x0, wl.center, wl.size), n_subsets=wl.subsets)
+    osem.step()
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(wl.iterations):
+        osem.step()
+    s1.record()
+    torch.cuda.synchronize()
+    osem_ms = s0.elapsed_time(s1) / wl.iterations
+
+    # roofline: per LOR 28 B record + 4 B out/value + 4 B (8 B) per visited voxel
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    alg = {"srf_siddon_projection": n * 32 + 4 * visits,
+           "srf_siddon_backprojection": n * 32 + 8 * visits}
+    roof = None
+    if kern:
+        dom = max(kern, key=lambda k: kern[k]["total_ms"])
+        per_launch = alg.get(dom, 0) * args.steps / max(kern[dom]["launches"], 1)
+        achieved = per_launch / (kern[dom]["mean_ms"] / 1e3) / 1e9
+        probe = profiling.measure_peaks()
+        t_meas = kern[dom]["total_ms"] / args.steps / 1e3
+        t_l2 = alg.get(dom, 0) / (probe["l2_gbs"] * 1e9)
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "peak_source": "measured hbm_gbs (burst copy)" if "hbm_gbs" in peaks
+                else "fallback hbm_gbs",
+                "algorithmic_bytes_per_launch": per_launch, "visited_voxels_per_step": visits,
+                "components": {"hbm": {"frac": achieved / hbm_peak},
+                               "l2": {"frac": t_l2 / t_meas, "peak_gbs": probe["l2_gbs"]},
+                               "sfu": {"frac": 0.0, "exps": 0}},
+                "kernel_ms": {k: {"launches": v["launches"], "mean_ms": v["mean_ms"]}
+                              for k, v in kern.items()}}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            base = siddon_cpu_baseline(events, model, image, args.cpu_seconds)
+        except Exception as exc:  # reported, never fatal for the GPU number
+            base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
+                    "sample": f"unavailable: {exc}"}
+    if rank == 0:
+        line = {"metric": METRICS["siddon64"], "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded events from a cylinder phantom)",
+                "config": {"workload": wl.name, "grid": list(wl.grid), "voxel_mm": wl.voxel,
+                           "events_per_rank": int(n), "tof_sigma2": 1.0e6,
+                           "parallelism": f"events sharded, {world} rank(s)",
+                           "l2": "image (0.5 MB) L2-resident; LOR records 28 MB per rank"},
+                "osem_iteration_ms": osem_ms,
+                "osem": {"subsets": wl.subsets, "iterations_timed": wl.iterations,
+                         "effmap_lors": 10_000_000},
+                "roofline": roof, "cpu_baseline": base, "e2e": e2e,
+                "gpu_launches": gpu_launches, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def siddon_cpu_baseline(events, model, image, target_s):
+    """The reference's host-built Siddon pair on all host threads over a bounded sample of
+    the same events. Rays the walk does not visit (they miss the image, or would make the
+    reference read outside it) are counted but not run: the reference returns 0 for them."""
+    from oracle import pyoracle as O
+    if not O.ReferenceHost.available():
+        raise RuntimeError("reference host build not present")
+    R = O.ReferenceHost()
+    threads = os.cpu_count() or 1
+    kimg, g, c, s = model.kernel_geometry(image)
+    img = kimg.cpu().numpy()
+    ev = events.cpu().numpy()
+    visits, _ = O.siddon_counts(np.ascontiguousarray(ev.T), g, c, s)
+
+    def run(k):
+        sel = np.ascontiguousarray(ev[:k][visits[:k] > 0].T)
+        t0 = time.perf_counter()
+        pv = R.siddon_projection(sel, img, g, c, s, model.tof_bin, model.tof_sigma2,
+                                 nthreads=threads)
+        R.siddon_backprojection(sel, pv, g, c, s, model.tof_bin, model.tof_sigma2,
+                                nthreads=threads)
+        return time.perf_counter() - t0
+
+    k = min(len(ev), 20000)
+    t = run(k)
+    k = int(min(len(ev), k * max(1.0, target_s / max(t, 1e-3))))
+    t = run(k)
+    return {"value": k / t, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"first {k} events ({int((visits[:k] > 0).sum())} visit the image), "
+                      f"projection + back-projection, {t:.1f} s wall"}
+
+
 # ------------------------------------------------------------------ reference arm
 
 
@@ -443,6 +633,8 @@ def main(argv=None):
         return run_reference(args)
     if args.workload == "batched96":
         return run_batched(args)
+    if args.workload == "siddon64":
+        return run_siddon(args)
 
     world, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)

@@ -198,6 +198,15 @@ int srf_siddon_backproject_adjoint(const float *x1, const float *y1, const float
                                    float tof_sigma2, float *image, int64_t num_events,
                                    int64_t lor_stride, int accumulate, void *stream);
 
+/* No counterpart in the reference: per-ray work of the Siddon operator, used for the
+ * roofline (algorithmic samples) and work estimation. counts[i] = voxels the ray's walk
+ * visits (the loop trips of RayTracing, siddon.cu.cc:293-331; 0 for a ray that misses the
+ * image). counts: DEVICE int32[N]. */
+int srf_siddon_count_samples(const float *x1, const float *y1, const float *z1, const float *x2,
+                             const float *y2, const float *z2, const int *grid,
+                             const float *center, const float *size, int *counts,
+                             int64_t num_events, int64_t lor_stride, void *stream);
+
 /* ------------------------------------------------------------------ LOR preprocessing
  * The reference runs these in host numpy; here they run on the device with the same
  * float32 arithmetic and the same output order (x group, y group, z group; in each,

@@ -21,7 +21,7 @@
 namespace srf {
 namespace {
 
-enum SiddonOp { kProj = 0, kBack = 1, kMap = 2, kAdj = 3 };
+enum SiddonOp { kProj = 0, kBack = 1, kMap = 2, kAdj = 3, kCount = 4 };
 
 struct SiddonParams {
     const float *x1, *y1, *z1, *x2, *y2, *z2, *tof;
@@ -36,6 +36,7 @@ struct SiddonParams {
     const float *values;
     float *image_out;
     float *proj_out;
+    int *count_out;  // kCount: voxels the walk visits per ray
 };
 
 // ClipRay (siddon.cu.cc:118-153) for one axis.
@@ -122,6 +123,7 @@ __global__ void __launch_bounds__(256) siddon_kernel(const SiddonParams p) {
         through = through && (tmin < tmax);
 
         float acc = 0.0f;
+        int n_visits = 0;
         if (through) {
             // SetupRayCast (siddon.cu.cc:261-284).
             int pos[3], step[3], in_buf[3];
@@ -144,7 +146,7 @@ __global__ void __launch_bounds__(256) siddon_kernel(const SiddonParams p) {
             const float weight = (OP == kMap) ? __fdiv_rn(1.0f, __fmul_rn(length, length))
                                               : __fdiv_rn(__fdiv_rn(1.0f, length), length);
             float t_tof = 0.0f;
-            const bool tof = (OP != kMap) && p.tof_on;
+            const bool tof = (OP != kMap && OP != kCount) && p.tof_on;
             if (tof)
                 t_tof = __double2float_rn((double)length * 0.5 - (double)tmin -
                                           (double)__ldg(p.tof + o));
@@ -172,7 +174,9 @@ __global__ void __launch_bounds__(256) siddon_kernel(const SiddonParams p) {
                 } else {
                     val = __fmul_rn(weight, l_len);
                 }
-                if (use) {
+                if (OP == kCount) {
+                    n_visits++;
+                } else if (use) {
                     if (OP == kProj) {
                         acc = fmaf(__ldg(p.image_in + mi), val, acc);
                     } else {
@@ -196,6 +200,7 @@ __global__ void __launch_bounds__(256) siddon_kernel(const SiddonParams p) {
             }
         }
         if (OP == kProj) p.proj_out[t] = acc;
+        if (OP == kCount) p.count_out[t] = n_visits;
     }
 }
 
@@ -329,4 +334,19 @@ extern "C" int srf_siddon_backproject_adjoint(const float *x1, const float *y1,
     p.values = values;
     p.image_out = image;
     return siddon_launch<kAdj>(p, (cudaStream_t)stream);
+}
+
+extern "C" int srf_siddon_count_samples(const float *x1, const float *y1, const float *z1,
+                                        const float *x2, const float *y2, const float *z2,
+                                        const int *grid, const float *center, const float *size,
+                                        int *counts, int64_t num_events, int64_t lor_stride,
+                                        void *stream) {
+    SiddonParams p{};
+    int st = siddon_setup(p, grid, center, size, 1.0f, 1.0e6f, num_events, lor_stride);
+    if (st != SRF_OK) return st;
+    if (num_events > 0 && (!x1 || !y1 || !z1 || !x2 || !y2 || !z2 || !counts))
+        return SRF_ERR_INVALID_ARGUMENT;
+    p.x1 = x1; p.y1 = y1; p.z1 = z1; p.x2 = x2; p.y2 = y2; p.z2 = z2;
+    p.count_out = counts;
+    return siddon_launch<kCount>(p, (cudaStream_t)stream);
 }

@@ -214,6 +214,18 @@ def tor_count_samples(lors, grid, center, size, kernel_width, geo_sigma2_flag=Fa
 # -------------------------------------------------------------------------- Siddon
 
 
+def siddon_count_samples(lors, grid, center, size, layout="auto"):
+    """Per-ray voxels visited by the Siddon walk (int32 [N]): the operator's work."""
+    dev = _check_cuda(lors)
+    t, cols, n, stride = _columns(lors, SIDDON_COLS, layout, min_cols=6)
+    g, ga, ca, sa = _geom(grid, center, size)
+    counts = torch.empty(n, dtype=torch.int32, device=dev)
+    with torch.cuda.device(dev):
+        _call(dev, "srf_siddon_count_samples", *cols[:6], ga, ca, sa, counts.data_ptr(), n,
+              stride, _stream(dev))
+    return counts
+
+
 def siddon_projection(lors, image, grid, center, size, tof_bin=1.0e4, tof_sigma2=1.0e4,
                       layout="auto", out=None):
     dev = _check_cuda(lors, image, out)

@@ -437,3 +437,14 @@ def test_slab_chunks_equal_one_pass():
     for a, b_ in zip(one, chunked):
         assert np.count_nonzero(a) > 0
         assert K.rel_l2(b_, a) <= 1e-6
+
+
+def test_siddon_count_samples_match_oracle():
+    """Per-ray voxel visits of the Siddon walk equal the oracle's count (rays that miss
+    the image, or start off the grid, visit none)."""
+    sc = K.siddon_case(n=20000, seed=67, grid=(64, 64, 32), voxel=3.4)
+    args = (sc["grid"], sc["center"], sc["size"])
+    visits, _ = O.siddon_counts(sc["lors"], *args)
+    got = host(ops.siddon_count_samples(cu(sc["lors"]), *args, layout="cn"))
+    assert visits.sum() > 0
+    np.testing.assert_array_equal(got.astype(np.int64), visits)
