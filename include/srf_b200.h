@@ -257,6 +257,14 @@ int srf_map_process(const float *lors, int64_t num_lors, int64_t lor_stride, flo
 int srf_mlem_update(float *image, const float *effinv, const float *bp, int64_t num_voxels,
                     void *stream);
 
+/* Sparse transaxial PSF of the PSF reconstruction step (PSFReconStep,
+ * src/python/srf/model/recon_step.py:56-115, there tf.sparse_tensor_dense_matmul):
+ * y = A x, A an [nrows, ncols] CSR matrix (rowptr int64[nrows+1], col int32, val float32),
+ * x a dense row-major [ncols, nz] matrix, y [nrows, nz] (y += A x with accumulate != 0).
+ * All DEVICE pointers. The adjoint is the same call with the CSR of A^T. */
+int srf_csr_spmm(const int64_t *rowptr, const int *col, const float *val, int64_t nrows,
+                 int64_t ncols, const float *x, int nz, float *y, int accumulate, void *stream);
+
 /* ------------------------------------------------------------------------ peak probes */
 
 /* No counterpart in the reference: measurement kernels for the roofline denominators
