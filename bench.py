@@ -76,6 +76,8 @@ def parse_args(argv=None):
                          "batched96: 64-frame "
                          "batched OSEM iteration vs the plain per-frame loop")
     ap.add_argument("--frames", type=int, default=64)
+    ap.add_argument("--no-effmap", dest="effmap", action="store_false",
+                    help="skip timing the efficiency-map pass (random detector pairs)")
     ap.add_argument("--tuning", default=None,
                     help="PATH,SLAB_SLICES,GRID_MULT for srf_tor_set_tuning (default: the "
                          "library's automatic choice)")
@@ -135,8 +137,12 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # the timed region starts once sampling runs (nvidia-smi takes a moment)
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
@@ -728,6 +734,29 @@ def main(argv=None):
                "path": "pinned host events -> recon_process -> projection -> backprojection "
                        "-> host image"}
 
+    # ---------------------------------------------------------------- effmap pass
+    effmap = None
+    if args.effmap:
+        from srf_b200 import recon
+        from srf_b200.synthetic import RandomLorSource
+        args_e = (list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
+                  wl.scanner.axial_length)
+        recon.efficiency_map(model, RandomLorSource(16_000_000, wl.scanner, 78, device=dev),
+                             *args_e)  # warm-up: one full chunk (sizes the scratch pool)
+        src = RandomLorSource(wl.n_effmap, wl.scanner, 77, device=dev)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        recon.efficiency_map(model, src, *args_e)
+        e1.record()
+        torch.cuda.synchronize()
+        e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        effmap = {"lors": wl.n_effmap, "ms": e_ms, "lors_per_s": wl.n_effmap / (e_ms / 1e3),
+                  "chunk": src.chunk,
+                  "path": "random crystal pairs generated on the device per chunk -> "
+                          "map_process -> TOR maplors of each axis group -> crop, normalise, "
+                          "invert"}
+
     # ---------------------------------------------------------------- roofline
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -788,7 +817,7 @@ def main(argv=None):
                                  % (n_lors * 40 // 10**6),
                            "tuning": args.tuning or "automatic"},
                 "roofline": roof, "cpu_baseline": base, "e2e": e2e,
-                "gpu_launches": gpu_launches, "clocks": clk}
+                "gpu_launches": gpu_launches, "clocks": clk, "effmap": effmap}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -87,15 +87,25 @@ def make_subsets(data, n_subsets):
 
 def efficiency_map(model, lors, grid, center, size, inner_radius, axial_length,
                    chunk=16_000_000, crop_ratio=0.95, threshold=1e-6, zero_below=True):
-    """Inverted efficiency map from detector-pair LORs ([N, 6] CUDA tensor or a callable
-    returning chunks): Maplors summed over the axis groups (or Siddon map), cropped,
-    normalised to max 1 and inverted (merge_map.py:37-41)."""
-    dev = lors.device
+    """Inverted efficiency map from detector-pair LORs: Maplors summed over the axis
+    groups (or Siddon map), cropped, normalised to max 1 and inverted
+    (merge_map.py:37-41). ``lors`` is an [N, 6] CUDA tensor, or a source with ``len()``
+    and ``source(start, count)`` returning [count, 6] CUDA chunks (for example
+    ``synthetic.RandomLorSource``), so that N LORs never exist at once; its chunk size
+    then sets ``chunk``."""
+    if callable(lors):
+        n = len(lors)
+        chunk = getattr(lors, "chunk", chunk)
+        dev = getattr(lors, "device", torch.device("cuda"))
+        take = lors
+    else:
+        n = lors.shape[0]
+        dev = lors.device
+        take = lambda s, c: lors[s:s + c]  # noqa: E731
     total = torch.zeros(tuple(grid), dtype=torch.float32, device=dev)
     img = Image(total, center, size)
-    n = lors.shape[0]
     for s in range(0, n, chunk):
-        part = lors[s:s + chunk]
+        part = take(s, min(chunk, n - s))
         if isinstance(model, SplitLoRsModel):
             groups = map_process(part)
             data = split_listmode(groups, without_tof=True)

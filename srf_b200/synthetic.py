@@ -188,6 +188,26 @@ def random_lors(n, scanner, seed, device="cpu"):
     return torch.cat([pos[i], pos[j]], 1).contiguous()
 
 
+class RandomLorSource:
+    """Random detector-pair LORs generated on the device chunk by chunk: chunk k of
+    ``chunk`` LORs is ``random_lors(count, scanner, seed * 1000003 + k)``, so any chunk
+    can be regenerated on its own and a pass over n LORs never holds more than one chunk.
+    Call as ``source(start, count)`` with ``start`` a multiple of ``chunk``."""
+
+    def __init__(self, n, scanner, seed, chunk=16_000_000, device="cuda"):
+        self.n, self.scanner, self.seed, self.chunk = int(n), scanner, int(seed), int(chunk)
+        self.device = torch.device(device)
+
+    def __len__(self):
+        return self.n
+
+    def __call__(self, start, count):
+        if start % self.chunk or count > self.chunk:
+            raise ValueError("chunks start at multiples of the chunk size")
+        return random_lors(count, self.scanner, self.seed * 1000003 + start // self.chunk,
+                           self.device)
+
+
 # --------------------------------------------------------------- named workloads
 
 

@@ -311,3 +311,23 @@ def test_unrolled_osem_checkpointing(small):
                    Image(cu(np.ones(grid, np.float32)), [0, 0, 0], size))
     o.run(5)
     assert K.rel_l2(outs[0][0], o.x.data.cpu().numpy()) < 1e-5
+
+
+def test_effmap_from_chunked_source_equals_tensor_input():
+    """The effmap pass over an on-device chunk source equals the pass over the same LORs
+    held as one tensor."""
+    from srf_b200 import SplitLoRsModel
+    from srf_b200 import recon
+    from srf_b200.synthetic import RandomLorSource
+    from tests import _cases as K
+    grid, voxel = (32, 32, 16), 6.4
+    size = [g * voxel for g in grid]
+    model = SplitLoRsModel(K.KW_CONFIG, False)
+    src = RandomLorSource(250_000, K.SCANNER, 5, chunk=100_000)
+    whole = torch.cat([src(s, min(src.chunk, len(src) - s))
+                       for s in range(0, len(src), src.chunk)])
+    args = (list(grid), [0, 0, 0], size, K.SCANNER.inner_radius, K.SCANNER.axial_length)
+    _, a = recon.efficiency_map(model, src, *args)
+    _, b = recon.efficiency_map(model, whole, *args, chunk=100_000)
+    assert torch.count_nonzero(b) > 0
+    assert float((a - b).norm() / b.norm()) < 1e-6
