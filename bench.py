@@ -68,12 +68,13 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--workload", default="tor128",
-                    choices=["tor128", "large256", "siddon64", "batched96"],
+                    choices=["tor128", "large256", "siddon64", "batched96", "autograd128"],
                     help="tor128: the headline TOF-TOR pair (default); large256: the same "
                          "pair on one 16M-event chunk of the large axial FOV workload "
                          "(256x256x128 at 2.5 mm, 1 m axial, 400 ps); siddon64: the plain "
                          "non-TOF Siddon pair and OSEM iteration (64x64x32, 1M events); "
-                         "batched96: 64-frame "
+                         "autograd128: forward + backward of 5 unrolled OSEM iterations "
+                         "(128x128x64, 8 frames x 5M events); batched96: 64-frame "
                          "batched OSEM iteration vs the plain per-frame loop")
     ap.add_argument("--frames", type=int, default=64)
     ap.add_argument("--no-effmap", dest="effmap", action="store_false",
@@ -507,6 +508,76 @@ def siddon_cpu_baseline(events, model, image, target_s):
                       f"projection + back-projection, {t:.1f} s wall"}
 
 
+def run_autograd(args):
+    """Differentiable projector at full size: 128x128x64 (3.2 mm), 8 frames of 5M events
+    (TOF 530 ps). Per frame, loss = sum_i ((A x_5)_i - log (A x_5)_i) + 0.01/2 * quadratic
+    6-neighbour penalty of x_5, with x_5 five unrolled MLEM iterations of x0 under
+    torch.utils.checkpoint; timed: forward + backward (gradient w.r.t. x0) of all frames.
+    Also the adjoint identity <A x, y> = <x, A^T y> of the autograd pair at this size."""
+    from srf_b200 import Image, SplitLoRsModel
+    from srf_b200 import preprocess as PP
+    from srf_b200 import synthetic as S
+    from srf_b200.autograd import Projector, poisson_nll, quadratic_penalty, unrolled_osem
+    from srf_b200.scanner import tof_info
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    wl = S.tor_128()
+    b, s2 = tof_info(wl.tof_res_ps, wl.tof_bin_ps)
+    model = SplitLoRsModel(wl.kernel_width, False, tof_sigma2=s2, tof_bin=b)
+    n_frames, n_ev = max(1, args.frames if args.frames != 64 else 8), args.events or 5_000_000
+    projs = []
+    for f in range(n_frames):
+        ph = S.random_phantom(4000 + f, wl.scanner.axial_length / 2)
+        ev = S.generate_events(n_ev, wl.scanner, ph, seed=4000 + f,
+                               tof_sigma_mm=math.sqrt(s2), device=dev)
+        data = PP.split_listmode(PP.recon_process(ev, wl.tof_res_ps))
+        projs.append(Projector(model, data, list(wl.grid), wl.center, wl.size))
+        del ev
+    x0 = (torch.rand(wl.grid, device=dev) + 0.5).requires_grad_(True)
+    effinv = torch.rand(wl.grid, device=dev) + 0.5
+
+    def step():
+        x0.grad = None
+        total = 0.0
+        for A in projs:
+            xk = unrolled_osem(A, x0, effinv, n_iterations=5, checkpoint=True)
+            loss = poisson_nll(A.forward(xk), per_event=True) + quadratic_penalty(xk, 0.01)
+            loss.backward()
+            total += float(loss.detach())
+        return total
+
+    step()  # warm-up
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    steps = max(1, args.steps // 5)
+    for _ in range(steps):
+        step()
+    s1.record()
+    torch.cuda.synchronize()
+    ms = s0.elapsed_time(s1) / steps
+    finite = bool(torch.isfinite(x0.grad).all())
+
+    # adjoint identity of the autograd pair on the first frame at full size
+    A = projs[0]
+    with torch.no_grad():
+        x = torch.rand(wl.grid, device=dev, dtype=torch.float32)
+        p = A.forward(x)
+        y = {a: torch.rand_like(v) for a, v in p.items()}
+        lhs = sum(float((p[a].double() * y[a].double()).sum()) for a in p)
+        rhs = float((x.double() * A.adjoint(y).double()).sum())
+    line = {"metric": "differentiable unrolled OSEM forward+backward time (128x128x64, "
+                      f"{n_frames} frames x {n_ev // 10**6}M events, 5 iterations)",
+            "value": ms, "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+            "steps": steps, "frames": n_frames, "events_per_frame": n_ev,
+            "adjoint_identity_rel_err": abs(lhs - rhs) / abs(lhs), "gradient_finite": finite,
+            "data": "synthetic (seeded per-frame phantoms)",
+            "config": {"workload": "autograd_128x128x64_8x5M", "grid": list(wl.grid),
+                       "voxel_mm": wl.voxel, "checkpoint": True, "beta": 0.01}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ reference arm
 
 
@@ -674,6 +745,8 @@ def main(argv=None):
         return run_batched(args)
     if args.workload == "siddon64":
         return run_siddon(args)
+    if args.workload == "autograd128":
+        return run_autograd(args)
 
     world, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
