@@ -77,6 +77,9 @@ def parse_args(argv=None):
                          "(128x128x64, 8 frames x 5M events); batched96: 64-frame "
                          "batched OSEM iteration vs the plain per-frame loop")
     ap.add_argument("--frames", type=int, default=64)
+    ap.add_argument("--no-order", dest="order", action="store_false",
+                    help="keep the preprocessed records in recon_process order instead of "
+                         "grouping similar directions (preprocess.order_by_direction)")
     ap.add_argument("--no-effmap", dest="effmap", action="store_false",
                     help="skip timing the efficiency-map pass (random detector pairs)")
     ap.add_argument("--tuning", default=None,
@@ -761,6 +764,9 @@ def main(argv=None):
     n_events = events.shape[0]
     model = model_for(wl, tof_bin, tof_sigma2)
     groups = PP.recon_process(events, wl.tof_res_ps)
+    groups_in = groups  # recon_process order: the CPU baseline samples the head of each group
+    if args.order:
+        groups = PP.order_by_direction(groups)
     data = PP.split_listmode(groups)
     image = Image(torch.as_tensor(img_np, device=dev), wl.center, wl.size)
     n_lors = sum(data[a].lors.shape[0] for a in "xyz")
@@ -814,6 +820,8 @@ def main(argv=None):
 
         def compute(ev):
             g = PP.recon_process(ev, wl.tof_res_ps)
+            if args.order:
+                g = PP.order_by_direction(g)
             d = PP.split_listmode(g)
             p = projection(model, image, d)
             bp = backprojection(model, p, image)
@@ -893,7 +901,7 @@ def main(argv=None):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            gh = {a: groups[a].cpu().numpy() for a in "xyz"}
+            gh = {a: groups_in[a].cpu().numpy() for a in "xyz"}
             base = cpu_baseline(gh, wl, tof_bin, tof_sigma2, img_np, args.cpu_seconds)
         except Exception as exc:  # reported, never fatal for the GPU number
             base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",

@@ -245,6 +245,16 @@ int srf_recon_process(const float *events, int64_t num_events, int64_t event_str
 int srf_recon_process_noalloc(const float *events, int64_t num_events, int64_t event_stride,
                               double tof_res, float *out, int64_t *group_counts, void *stream);
 
+/* No counterpart in the reference: an optional step between preprocessing and the TOR
+ * projectors. Copies records [num_records, ncols] (row-major, record_stride floats apart,
+ * ncols >= 6: x1,y1,z1,x2,y2,z2 first) to `out` (same layout, must not alias `records`)
+ * reordered inside each block of 4096 consecutive records by the shape of the LOR's tube
+ * section (a stable sort on a quantised direction class). Records keep their block;
+ * list-mode events being an unordered set, reconstructing from `out` gives the same sums
+ * in another order, with fewer voxel slots walked by the slab kernels. */
+int srf_order_by_direction(const float *records, int64_t num_records, int ncols,
+                           int64_t record_stride, float *out, void *stream);
+
 /* Replaces map_process, on_tor_lors.py:243-248: lors [N, >=6] -> out [N, 7] rows
  * (p1, p2 with the dominant axis last, sigma2_factor). */
 int srf_map_process(const float *lors, int64_t num_lors, int64_t lor_stride, float *out,

@@ -55,6 +55,7 @@ SIGNATURES = {
     "srf_map_process": ([_p, _i64, _i64, _p, _p, _p, _i64, _p], _int),
     "srf_recon_process_noalloc": ([_p, _i64, _i64, C.c_double, _p, _p, _p], _int),
     "srf_csr_spmm": ([_p, _p, _p, _i64, _i64, _p, _int, _p, _int, _p], _int),
+    "srf_order_by_direction": ([_p, _i64, _int, _i64, _p, _p], _int),
     "srf_probe_threads": ([_p], _int),
     "srf_probe_l2_read": ([_p, _i64, _int, _p, _p], _int),
     "srf_probe_ex2": ([_int, _p, _p], _int),

@@ -59,10 +59,13 @@ class BatchedOSEM:
     ``effinv``: Image (inverted efficiency map, shared by all frames); ``x0``: [F,nx,ny,nz]
     CUDA tensor (or one [nx,ny,nz] image replicated); center/size from ``effinv``."""
 
-    def __init__(self, model, frames, effinv, x0, n_subsets=1, use_graph=False):
+    def __init__(self, model, frames, effinv, x0, n_subsets=1, use_graph=False, order=True):
         if not isinstance(model, SplitLoRsModel):
             raise TypeError("BatchedOSEM runs the TOR model (SplitLoRsModel)")
         self.model = model
+        if order:  # once per reconstruction, as srf_b200.recon.OSEM does
+            from .preprocess import order_by_direction
+            frames = [order_by_direction(g) for g in frames]
         self.batch = FrameBatch(frames, n_subsets)
         self.F = self.batch.n_frames
         self.S = self.batch.n_subsets

@@ -1,0 +1,79 @@
+// Reordering of preprocessed LOR records by the shape of their tube's section, inside
+// blocks of 4096 consecutive records (no counterpart in the reference; an optional step
+// between preprocessing and the projectors).
+//
+// A record's section box spans sqrt((1 - uy^2)/q) by sqrt((1 - ux^2)/q), q = 1 - ux^2 - uy^2,
+// with (ux, uy) the in-slice components of its unit direction. The slab kernels hand a
+// warp 32 consecutive LORs of a slab and walk the largest box among them, so records of
+// similar direction side by side walk fewer voxel slots. Sorting only inside blocks keeps
+// every stretch of the per-slab lists a mix of directions, so the persistent grid's equal
+// shares stay equal work. The class key quantises both extents to 16 levels over [1, 2)
+// (dominant-axis groups have extents in [1, sqrt(3)]); records with NaN sort last. The sort
+// is a stable block radix sort, so the order is deterministic.
+
+#include <cub/block/block_radix_sort.cuh>
+
+#include "srf_common.cuh"
+
+namespace srf {
+namespace {
+
+constexpr int kOrderThreads = 512;
+constexpr int kOrderItems = 8;
+constexpr int kOrderBlock = kOrderThreads * kOrderItems;  // 4096 records
+
+__device__ __forceinline__ int direction_class(const float *r) {
+    const float dx = r[3] - r[0], dy = r[4] - r[1], dz = r[5] - r[2];
+    const float inv = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
+    const float ux2 = dx * dx * inv * inv, uy2 = dy * dy * inv * inv;
+    const float q = fmaxf(1.0f - ux2 - uy2, 1e-6f);
+    const float bx = sqrtf((1.0f - uy2) / q), by = sqrtf((1.0f - ux2) / q);
+    if (!(bx == bx) || !(by == by)) return 255;
+    const int kx = min(15, max(0, (int)((bx - 1.0f) * 16.0f)));
+    const int ky = min(15, max(0, (int)((by - 1.0f) * 16.0f)));
+    return kx * 16 + ky;
+}
+
+__global__ void __launch_bounds__(kOrderThreads)
+order_kernel(const float *__restrict__ in, float *__restrict__ out, int64_t n, int ncols,
+             int64_t stride) {
+    using Sort = cub::BlockRadixSort<int, kOrderThreads, kOrderItems, int>;
+    __shared__ typename Sort::TempStorage tmp;
+    const int64_t base = (int64_t)blockIdx.x * kOrderBlock;
+    int key[kOrderItems], idx[kOrderItems];
+#pragma unroll
+    for (int k = 0; k < kOrderItems; k++) {
+        const int j = threadIdx.x * kOrderItems + k;  // blocked arrangement: stable order
+        const int64_t t = base + j;
+        idx[k] = j;
+        key[k] = t < n ? direction_class(in + t * stride) : 256;  // padding sorts last
+    }
+    Sort(tmp).Sort(key, idx, 0, 9);
+#pragma unroll
+    for (int k = 0; k < kOrderItems; k++) {
+        const int j = threadIdx.x * kOrderItems + k;
+        const int64_t dst = base + j;
+        if (dst >= n) continue;
+        const float *src = in + (base + idx[k]) * stride;
+        float *d = out + dst * stride;
+        for (int c = 0; c < ncols; c++) d[c] = src[c];
+    }
+}
+
+}  // namespace
+}  // namespace srf
+
+using namespace srf;
+
+extern "C" int srf_order_by_direction(const float *records, int64_t num_records, int ncols,
+                                      int64_t record_stride, float *out, void *stream) {
+    if (num_records < 0 || ncols < 6 || record_stride < ncols) return SRF_ERR_INVALID_ARGUMENT;
+    if (num_records == 0) return SRF_OK;
+    if (!records || !out || records == out) return SRF_ERR_INVALID_ARGUMENT;
+    const int64_t blocks = (num_records + kOrderBlock - 1) / kOrderBlock;
+    if (blocks > INT32_MAX) return SRF_ERR_UNSUPPORTED;
+    order_kernel<<<(int)blocks, kOrderThreads, 0, (cudaStream_t)stream>>>(
+        records, out, num_records, ncols, record_stride);
+    count_launches(1);
+    return check_launch();
+}

@@ -107,3 +107,43 @@ def initial_image(grid, center, size, inner_radius, axial_length, device, crop_r
     keep = torch.as_tensor(crop_mask(grid, center, size, inner_radius, axial_length,
                                      crop_ratio), device=device)
     return keep.to(torch.float32)
+
+
+def order_by_direction(groups):
+    """Reorder each axis group's [N, C] records (C >= 6, x1..z2 first) by the shape of their
+    tube's section, inside blocks of 4096 consecutive records (``srf_order_by_direction``).
+
+    A LOR's section box spans sqrt((1 - uy^2) / q) by sqrt((1 - ux^2) / q) (q = 1 - ux^2 -
+    uy^2, (ux, uy) its in-slice direction in the kernel frame), so records of similar
+    direction walk boxes of the same size. The slab kernels give a warp 32 consecutive
+    LORs of a slab and walk the largest box among them; grouping similar directions makes
+    that box smaller, while sorting only inside blocks keeps every stretch of the per-slab
+    lists a mix of directions (equal shares of the persistent grid stay equal work).
+    List-mode events form an unordered set, and projection values follow their records,
+    so a reconstruction over the reordered groups is the same sum taken in another order.
+    Returns new groups (same device)."""
+    out = {}
+    for a, g in groups.items():
+        if g.shape[0] < 2:
+            out[a] = g
+            continue
+        src = g.to(torch.float32).contiguous()
+        dst = torch.empty_like(src)
+        dev = src.device
+        with torch.cuda.device(dev):
+            _lib.call("srf_order_by_direction", src.data_ptr(), src.shape[0], src.shape[1],
+                      src.stride(0), dst.data_ptr(), _stream(dev))
+        out[a] = dst
+    return out
+
+
+def order_listmode(data):
+    """``order_by_direction`` for a ListModeDataSplit: each group's records reordered with
+    their values (the values travel as an extra column)."""
+    out = []
+    for a in ("x", "y", "z"):
+        d = data[a]
+        rec = torch.cat([d.lors.to(torch.float32), d.values.to(torch.float32).reshape(-1, 1)], 1)
+        o = order_by_direction({a: rec})[a]
+        out.append(type(d)(o[:, :-1].contiguous(), o[:, -1].contiguous()))
+    return type(data)(*out)

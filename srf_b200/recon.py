@@ -125,11 +125,17 @@ class OSEM:
     """Ordered-subsets EM with optional CUDA-graph capture of each iteration.
 
     ``data``: ListModeDataSplit (TOR) or ListModeData (Siddon) with values of one.
-    ``effinv``: inverted efficiency map (Image). ``x0``: initial image (Image)."""
+    ``effinv``: inverted efficiency map (Image). ``x0``: initial image (Image).
+    ``order``: reorder the TOR records once by direction (``preprocess.order_listmode``)
+    so that every iteration's slab kernels walk fewer voxel slots; the image is the same
+    sum over the events taken in another order."""
 
-    def __init__(self, model, data, effinv, x0, n_subsets=1, use_graph=False):
+    def __init__(self, model, data, effinv, x0, n_subsets=1, use_graph=False, order=True):
         self.model = model
         self.n_subsets = int(n_subsets)
+        if order and isinstance(model, SplitLoRsModel):
+            from .preprocess import order_listmode
+            data = order_listmode(data)
         self.subsets = make_subsets(data, self.n_subsets)
         self.effinv = Image((effinv.data * float(self.n_subsets)).contiguous(), effinv.center,
                             effinv.size)
