@@ -249,7 +249,8 @@ int srf_recon_process_noalloc(const float *events, int64_t num_events, int64_t e
  * projectors. Copies records [num_records, ncols] (row-major, record_stride floats apart,
  * ncols >= 6: x1,y1,z1,x2,y2,z2 first) to `out` (same layout, must not alias `records`)
  * reordered inside each block of 4096 consecutive records by the shape of the LOR's tube
- * section (a stable sort on a quantised direction class). Records keep their block;
+ * section, then by where it starts along the slice axis (a stable sort on a quantised
+ * key). Records keep their block;
  * list-mode events being an unordered set, reconstructing from `out` gives the same sums
  * in another order, with fewer voxel slots walked by the slab kernels. */
 int srf_order_by_direction(const float *records, int64_t num_records, int ncols,

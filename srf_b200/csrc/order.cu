@@ -8,8 +8,10 @@
 // similar direction side by side walk fewer voxel slots. Sorting only inside blocks keeps
 // every stretch of the per-slab lists a mix of directions, so the persistent grid's equal
 // shares stay equal work. The class key quantises both extents to 16 levels over [1, 2)
-// (dominant-axis groups have extents in [1, sqrt(3)]); records with NaN sort last. The sort
-// is a stable block radix sort, so the order is deterministic.
+// (dominant-axis groups have extents in [1, sqrt(3)]); inside a class, records are ordered
+// by where the LOR starts along the slice axis (8 mm bins), so a warp's segments cover
+// similar slice counts. Records with NaN sort last. The sort is a stable block radix sort,
+// so the order is deterministic.
 
 #include <cub/block/block_radix_sort.cuh>
 
@@ -28,10 +30,13 @@ __device__ __forceinline__ int direction_class(const float *r) {
     const float ux2 = dx * dx * inv * inv, uy2 = dy * dy * inv * inv;
     const float q = fmaxf(1.0f - ux2 - uy2, 1e-6f);
     const float bx = sqrtf((1.0f - uy2) / q), by = sqrtf((1.0f - ux2) / q);
-    if (!(bx == bx) || !(by == by)) return 255;
+    if (!(bx == bx) || !(by == by)) return 255 << 8;
     const int kx = min(15, max(0, (int)((bx - 1.0f) * 16.0f)));
     const int ky = min(15, max(0, (int)((by - 1.0f) * 16.0f)));
-    return kx * 16 + ky;
+    // secondary: where the LOR starts along the slice axis (8 mm bins over +-1 m)
+    const float zs = fminf(r[2], r[5]);
+    const int kz = (zs == zs) ? min(255, max(0, (int)((zs + 1024.0f) * 0.125f))) : 255;
+    return ((kx * 16 + ky) << 8) | kz;
 }
 
 __global__ void __launch_bounds__(kOrderThreads)
@@ -46,9 +51,9 @@ order_kernel(const float *__restrict__ in, float *__restrict__ out, int64_t n, i
         const int j = threadIdx.x * kOrderItems + k;  // blocked arrangement: stable order
         const int64_t t = base + j;
         idx[k] = j;
-        key[k] = t < n ? direction_class(in + t * stride) : 256;  // padding sorts last
+        key[k] = t < n ? direction_class(in + t * stride) : (256 << 8);  // padding sorts last
     }
-    Sort(tmp).Sort(key, idx, 0, 9);
+    Sort(tmp).Sort(key, idx, 0, 17);
 #pragma unroll
     for (int k = 0; k < kOrderItems; k++) {
         const int j = threadIdx.x * kOrderItems + k;
