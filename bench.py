@@ -883,8 +883,8 @@ def main(argv=None):
         achieved = per_launch_bytes / (kern[dom]["mean_ms"] / 1e3) / 1e9
         traffic = None
         prof = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
-        if os.path.exists(prof):
-            traffic = json.load(open(prof)).get(dom)
+        if os.path.exists(prof):  # measured per workload; null where not captured
+            traffic = json.load(open(prof)).get(wl.name, {}).get(dom)
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
                 "peak_source": f"{peak_src} hbm_gbs (burst copy)",
