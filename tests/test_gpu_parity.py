@@ -7,6 +7,7 @@ same operator. Set SRF_PARITY_LOG=<file> to append each measured error as JSON.
 """
 
 import json
+import math
 import os
 
 import numpy as np
@@ -448,3 +449,32 @@ def test_siddon_count_samples_match_oracle():
     got = host(ops.siddon_count_samples(cu(sc["lors"]), *args, layout="cn"))
     assert visits.sum() > 0
     np.testing.assert_array_equal(got.astype(np.int64), visits)
+
+
+# kernel widths whose window edge P = ceil((sqrt(2) kw + voxel_z) / voxel_x) covers every
+# specialised slab / LOR-centric kernel (P = 2..8) and the generic kernel (P > 8), at 3.2 mm
+KW_FOR_PATCH = {2: 2.0, 3: 4.0, 4: 6.0, 5: 8.0, 6: K.KW_CONFIG, 7: 12.5, 8: 15.0, 10: 20.0}
+
+
+@pytest.fixture(scope="module")
+def pcase():
+    return K.tor_case(n=4000, seed=37, grid=(96, 96, 48), voxel=3.2, n_box=800)
+
+
+@pytest.mark.parametrize("patch", list(KW_FOR_PATCH))
+def test_tor_every_window_size(pcase, patch, scatter_kernel):
+    """Projection and back-projection against the oracle for every window size."""
+    kw = KW_FOR_PATCH[patch]
+    assert math.ceil((math.sqrt(2) * np.float32(kw) + 3.2) / 3.2) == patch
+    b, s2 = K.tof_params(530.0)
+    for axis in "xz":
+        lors, img, g, c, s = K.tor_axis(pcase, axis)
+        pv = host(ops.tor_projection(cu(lors), cu(img), g, c, s, kw, False, b, s2, layout="cn"))
+        ref = O.tor_projection(lors, img, g, c, s, kw, False, b, s2, mode="f32", contract=True)
+        assert np.count_nonzero(ref) > 0
+        assert K.rel_l2(pv, ref) <= TOL, (axis, "projection")
+        bp = host(ops.tor_backprojection(cu(img), cu(lors), cu(ref), g, c, s, kw, False, b, s2,
+                                         layout="cn"))
+        refb = O.tor_backprojection(lors, ref, g, c, s, kw, False, b, s2, mode="f32",
+                                    contract=True)
+        assert K.rel_l2(bp, refb) <= TOL, (axis, "back-projection")
