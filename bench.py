@@ -350,8 +350,12 @@ def run_siddon(args):
     img_np = phantom.voxelize(wl.grid, wl.center, wl.size) + np.float32(0.05)
     image = Image(torch.as_tensor(img_np, device=dev), wl.center, wl.size)
     model = CompleteLoRsModel(tof_sigma2=1.0e6, tof_bin=1.0e4)
-    data = ListModeData(events, torch.ones(events.shape[0], device=dev))
     kimg, g, c, sz = model.kernel_geometry(image)
+    events_in = events  # generation order: the CPU baseline samples its head
+    if args.order:
+        from srf_b200.preprocess import order_rays_by_length
+        events = order_rays_by_length(events, g, c, sz)
+    data = ListModeData(events, torch.ones(events.shape[0], device=dev))
     visits = int(ops.siddon_count_samples(events, g, c, sz, layout="nc").sum(dtype=torch.int64))
 
     def step():
@@ -454,7 +458,7 @@ def run_siddon(args):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            base = siddon_cpu_baseline(events, model, image, args.cpu_seconds)
+            base = siddon_cpu_baseline(events_in, model, image, args.cpu_seconds)
         except Exception as exc:  # reported, never fatal for the GPU number
             base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
                     "sample": f"unavailable: {exc}"}
@@ -709,18 +713,23 @@ def run_batched(args):
     torch.cuda.synchronize()
     batched_ms = s0.elapsed_time(s1) / reps
 
-    plain = [recon.OSEM(model, PP.split_listmode(g), effinv, Image(x0, center, size),
-                        n_subsets=S_sub) for g in frames]
-    for o in plain:
-        o.step()
-    torch.cuda.synchronize()
-    s0.record()
-    for _ in range(reps):
+    # the plain per-frame loop at its faster setting (records ordered or not)
+    plain_by_order = {}
+    for order in (True, False):
+        plain = [recon.OSEM(model, PP.split_listmode(g), effinv, Image(x0, center, size),
+                            n_subsets=S_sub, order=order) for g in frames]
         for o in plain:
             o.step()
-    s1.record()
-    torch.cuda.synchronize()
-    plain_ms = s0.elapsed_time(s1) / reps
+        torch.cuda.synchronize()
+        s0.record()
+        for _ in range(reps):
+            for o in plain:
+                o.step()
+        s1.record()
+        torch.cuda.synchronize()
+        plain_by_order[order] = (s0.elapsed_time(s1) / reps, plain)
+    plain_order = min(plain_by_order, key=lambda k: plain_by_order[k][0])
+    plain_ms, plain = plain_by_order[plain_order]
     errs = []
     for f, o in enumerate(plain):
         a, b = bat.x[f].double(), o.x.data.double()
@@ -729,6 +738,7 @@ def run_batched(args):
     line = {"metric": "batched 64-frame TOF OSEM iteration time (96x96x48, 10 subsets)",
             "value": batched_ms, "unit": "ms", "higher_is_better": False, "n_gpus": 1,
             "plain_loop_ms": plain_ms, "speedup_vs_plain": plain_ms / batched_ms,
+            "plain_loop_ms_by_order": {str(k): v[0] for k, v in plain_by_order.items()},
             "iterations_timed": reps, "frames": args.frames, "events_total": n_events,
             "rel_l2_batched_vs_plain_max": max(errs), "autotuned": list(best),
             "autotune_ms": {str(k): v for k, v in (timings or {}).items()},

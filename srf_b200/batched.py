@@ -24,9 +24,11 @@ class FrameBatch:
 
     ``frames``: list of dicts {'x','y','z'} -> [N_f_a, 10] CUDA tensors (the output of
     ``recon_process`` per frame). Subset k of every frame holds its events k, k+S, ...
-    of each axis group (the interleaving of ``srf_b200.recon.make_subsets``)."""
+    of each axis group (the interleaving of ``srf_b200.recon.make_subsets``); with
+    ``order`` each frame's subset is then reordered for the kernels
+    (``preprocess.order_by_direction``), which changes summation order only."""
 
-    def __init__(self, frames, n_subsets=1):
+    def __init__(self, frames, n_subsets=1, order=False):
         self.n_frames = len(frames)
         self.n_subsets = int(n_subsets)
         self.subsets = []
@@ -36,6 +38,9 @@ class FrameBatch:
                 parts, ids = [], []
                 for f, g in enumerate(frames):
                     sub = g[a][k::self.n_subsets] if self.n_subsets > 1 else g[a]
+                    if order:
+                        from .preprocess import order_by_direction
+                        sub = order_by_direction({a: sub})[a]
                     parts.append(sub)
                     ids.append(torch.full((sub.shape[0],), f, dtype=torch.int32,
                                           device=sub.device))
@@ -63,10 +68,9 @@ class BatchedOSEM:
         if not isinstance(model, SplitLoRsModel):
             raise TypeError("BatchedOSEM runs the TOR model (SplitLoRsModel)")
         self.model = model
-        if order:  # once per reconstruction, as srf_b200.recon.OSEM does
-            from .preprocess import order_by_direction
-            frames = [order_by_direction(g) for g in frames]
-        self.batch = FrameBatch(frames, n_subsets)
+        # records reordered once per reconstruction inside each frame's subsets, as
+        # srf_b200.recon.OSEM does
+        self.batch = FrameBatch(frames, n_subsets, order=order)
         self.F = self.batch.n_frames
         self.S = self.batch.n_subsets
         grid = list(effinv.data.shape)

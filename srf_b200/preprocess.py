@@ -147,3 +147,25 @@ def order_listmode(data):
         o = order_by_direction({a: rec})[a]
         out.append(type(d)(o[:, :-1].contiguous(), o[:, -1].contiguous()))
     return type(data)(*out)
+
+
+def ray_length_order(events, grid, center, size, block=4096):
+    """Permutation that sorts [N, >=6] ray records by the number of voxels their Siddon walk
+    visits (``srf_siddon_count_samples``), inside blocks of ``block`` consecutive records,
+    so that the rays a warp walks together finish together. The geometry is the Siddon
+    op's kernel order (grid, center, size, x fastest)."""
+    from .ops import siddon_count_samples
+    ev = events.to(torch.float32).contiguous()
+    n = ev.shape[0]
+    if n < 2:
+        return torch.arange(n, device=ev.device)
+    visits = siddon_count_samples(ev, grid, center, size, layout="nc").to(torch.int64)
+    blk = torch.arange(n, device=ev.device, dtype=torch.int64) // int(block)
+    return torch.argsort(blk * (1 << 24) + visits, stable=True)
+
+
+def order_rays_by_length(events, grid, center, size, block=4096):
+    """Siddon counterpart of ``order_by_direction``: the records reordered by
+    ``ray_length_order`` (a reconstruction over them is the same sum in another order)."""
+    perm = ray_length_order(events, grid, center, size, block)
+    return events.to(torch.float32)[perm].contiguous()

@@ -82,6 +82,21 @@ def make_subsets(data, n_subsets):
     return out
 
 
+def order_subset(model, data, image):
+    """One subset's records reordered for the kernels (TOR: by direction inside 4096-record
+    blocks, ``preprocess.order_listmode``; Siddon: by walk length, ``preprocess.
+    ray_length_order``); values follow their records."""
+    if isinstance(model, SplitLoRsModel):
+        from .preprocess import order_listmode
+        return order_listmode(data)
+    if isinstance(model, CompleteLoRsModel) and len(data) > 1:
+        from .preprocess import ray_length_order
+        _, g, c, s = model.kernel_geometry(image)
+        perm = ray_length_order(data.lors, g, c, s)
+        return type(data)(data.lors[perm].contiguous(), data.values[perm].contiguous())
+    return data
+
+
 # ---------------------------------------------------------------------- efficiency map
 
 
@@ -126,17 +141,16 @@ class OSEM:
 
     ``data``: ListModeDataSplit (TOR) or ListModeData (Siddon) with values of one.
     ``effinv``: inverted efficiency map (Image). ``x0``: initial image (Image).
-    ``order``: reorder the TOR records once by direction (``preprocess.order_listmode``)
-    so that every iteration's slab kernels walk fewer voxel slots; the image is the same
-    sum over the events taken in another order."""
+    ``order``: reorder each subset's records once (``order_subset``) so that every
+    iteration's kernels waste fewer lanes; subset membership follows the caller's event
+    order, so the image is the same sums taken in another order."""
 
     def __init__(self, model, data, effinv, x0, n_subsets=1, use_graph=False, order=True):
         self.model = model
         self.n_subsets = int(n_subsets)
-        if order and isinstance(model, SplitLoRsModel):
-            from .preprocess import order_listmode
-            data = order_listmode(data)
         self.subsets = make_subsets(data, self.n_subsets)
+        if order:  # inside each subset: the subsets hold the caller's events k, k+S, ...
+            self.subsets = [order_subset(model, d, x0) for d in self.subsets]
         self.effinv = Image((effinv.data * float(self.n_subsets)).contiguous(), effinv.center,
                             effinv.size)
         self.x = Image(x0.data.clone().contiguous(), x0.center, x0.size)

@@ -366,3 +366,46 @@ def test_order_by_direction_permutes_within_blocks_and_keeps_the_reconstruction(
           for d in (PP.split_listmode(groups), PP.split_listmode(ordered))]
     assert torch.count_nonzero(bp[0]) > 0
     assert float((bp[1] - bp[0]).norm() / bp[0].norm()) < 1e-6
+
+
+def test_siddon_osem_ordered_equals_unordered():
+    """Ray ordering by walk length changes the summation order only."""
+    from srf_b200 import CompleteLoRsModel
+    from srf_b200.data import Image, ListModeData
+    from srf_b200.recon import OSEM
+    sc = K.siddon_case(n=30_000, seed=23, grid=(64, 64, 32), voxel=3.4)
+    model = CompleteLoRsModel(tof_sigma2=1.0e6, tof_bin=1.0e4)
+    lors = cu(np.ascontiguousarray(sc["lors"].T))
+    data = ListModeData(lors, torch.ones(lors.shape[0], device="cuda"))
+    grid = tuple(sc["grid"])
+    x0 = Image(torch.ones(grid, device="cuda"), sc["center"], sc["size"])
+    eff = Image(torch.rand(grid, device="cuda") + 0.5, sc["center"], sc["size"])
+    out = []
+    for order in (False, True):
+        o = OSEM(model, data, eff, x0, n_subsets=2, order=order)
+        o.step()
+        out.append(o.x.data)
+    assert float((out[1] - out[0]).norm() / out[0].norm()) < 1e-6
+
+
+def test_tor_osem_subsets_ordered_equals_unordered():
+    """Subsets hold the caller's events k, k+S, ...; ordering inside them changes the
+    summation order only."""
+    from srf_b200 import SplitLoRsModel
+    from srf_b200 import preprocess as PP
+    from srf_b200.data import Image
+    from srf_b200.recon import OSEM
+    grid, voxel = (64, 64, 32), 6.4
+    size = [g * voxel for g in grid]
+    ev = K.events(30_000, 29, 530.0).astype(np.float32)
+    data = PP.split_listmode(PP.recon_process(cu(ev), 530.0))
+    b, s2 = K.tof_params(530.0)
+    model = SplitLoRsModel(K.KW_CONFIG, False, tof_sigma2=s2, tof_bin=b)
+    x0 = Image(torch.ones(grid, device="cuda"), [0, 0, 0], size)
+    eff = Image(torch.rand(grid, device="cuda") + 0.5, [0, 0, 0], size)
+    out = []
+    for order in (False, True):
+        o = OSEM(model, data, eff, x0, n_subsets=3, order=order)
+        o.step()
+        out.append(o.x.data)
+    assert float((out[1] - out[0]).norm() / out[0].norm()) < 1e-6
