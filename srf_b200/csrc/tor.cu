@@ -629,6 +629,20 @@ __device__ __forceinline__ void lor_slab_ids(const TorParams &p, const SegPlan &
 }
 
 // kBand: sp.nbands > 1 (slab ids over slice ranges and row bands).
+// atomicAdd(&counter[id], 1) for the calling lane, with one shared-memory update per
+// distinct id among the warp's active lanes (neighbouring LORs mostly share slabs). Returns
+// the lane's slot: the counter's old value plus its rank among the lanes with that id.
+__device__ __forceinline__ int warp_increment(int *counter, int id) {
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, id);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int first = 0;
+    if (lane == leader) first = atomicAdd(counter + id, __popc(peers));
+    first = __shfl_sync(active, first, leader);
+    return first + __popc(peers & ((1u << lane) - 1u));
+}
+
 template <int OP, bool kBand>
 __global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams p, SegPlan sp) {
     extern __shared__ int hist[];  // [n_slabs]
@@ -718,7 +732,7 @@ __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p
         int s_lo = 0, s_hi = p.gz - 1;
         if (kBand) lor_slices(p, t, s_lo, s_hi);  // same range as seg_count's
         lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi, [&](int id) {
-            const int pos = atomicAdd(&cursor[id], 1);
+            const int pos = warp_increment(cursor, id);
             sp.seg[sp.slab_offs[id] + sp.tile_offs[(int64_t)blockIdx.x * sp.n_slabs + id] + pos] =
                 (int)t;
         });
