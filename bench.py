@@ -10,7 +10,8 @@ synthetic (no public dataset is involved) and preprocessed on the GPU by
 
 One step = the OSEM numerator pass the reference runs per iteration
 (model/recon_step.py:38-40): TOR projection of all three dominant-axis groups, then
-the reference's back-projection A^T(1/Ax) of all three groups into one image; with
+the reference's back-projection A^T(1/Ax) of all three groups into one image (one
+combined library call per group; ``--separate-ops`` makes the two calls); with
 N > 1 GPUs each rank owns its own 10M events (weak scaling) and the back-projected
 images are summed with one NCCL all-reduce.
 
@@ -21,9 +22,10 @@ images are summed with one NCCL all-reduce.
   copies the image back.
 * ``roofline``: the dominant op's algorithmic bytes per call (per LOR: the 40-byte
   record, 4 bytes of output or value, and 4 bytes per non-zero-weight voxel sample for
-  the projection, 8 for the back-projection's read-modify-write) over its CUDA-event
-  duration inside the timed region, against the measured HBM copy bandwidth; plus the
-  bound of the slowest of HBM, L2 and SFU (ex2) at their measured peaks.
+  the projection, 8 for the back-projection's read-modify-write; the combined call,
+  which runs both, counts both) over its CUDA-event duration inside the timed region,
+  against the measured HBM copy bandwidth; plus the bound of the slowest of HBM, L2 and
+  SFU (ex2) at their measured peaks.
 * ``cpu_baseline``: the reference's own projector sources compiled for the host
   (oracle/_ref), all host threads, on a bounded sample of the same LORs.
 
@@ -80,12 +82,24 @@ def parse_args(argv=None):
     ap.add_argument("--no-order", dest="order", action="store_false",
                     help="keep the preprocessed records in recon_process order instead of "
                          "grouping similar directions (preprocess.order_by_direction)")
+    ap.add_argument("--separate-ops", dest="combined", action="store_false",
+                    help="run projection and back-projection as two library calls (the "
+                         "reference's op sequence) instead of the combined TOR call")
     ap.add_argument("--no-effmap", dest="effmap", action="store_false",
                     help="skip timing the efficiency-map pass (random detector pairs)")
     ap.add_argument("--tuning", default=None,
                     help="PATH,SLAB_SLICES,GRID_MULT for srf_tor_set_tuning (default: the "
                          "library's automatic choice)")
     return ap.parse_args(argv)
+
+
+def project_back(model, image, data, combined=True):
+    """The step's projection then back-projection of the projected values (the reference
+    recon step's numerator); ``combined`` uses the one-call TOR entry point."""
+    from srf_b200 import backprojection, projection, projection_backprojection
+    if combined:
+        return projection_backprojection(model, image, data)[1]
+    return backprojection(model, projection(model, image, data), image)
 
 
 # ------------------------------------------------------------------ distributed
@@ -265,15 +279,18 @@ def roofline_components(kernel, ms_per_step, alg_bytes, n_lors, rec, useful, slo
     t_sfu = useful / probe["ex2_per_s"]
     t_meas = ms_per_step / 1e3
     bound = max(t_hbm, t_l2, t_sfu)
-    per = 8 if kernel == "srf_tor_backprojection" else 4
+    # bytes per window sample: image read (projection), read-modify-write (back-projection)
+    per = {"srf_tor_backprojection": 8, "srf_tor_projection_backprojection": 12}.get(kernel, 4)
+    lor_passes = 2 if kernel == "srf_tor_projection_backprojection" else 1
     return {
         "hbm": {"ms": t_hbm * 1e3, "frac": t_hbm / t_meas, "peak_gbs": hbm_peak},
         "l2": {"ms": t_l2 * 1e3, "frac": t_l2 / t_meas, "peak_gbs": probe["l2_gbs"]},
         "sfu": {"ms": t_sfu * 1e3, "frac": t_sfu / t_meas, "peak_ex2_per_s": probe["ex2_per_s"],
                 "exps": useful, "reference_exps": useful + slots},
         "bound_ms": bound * 1e3, "measured_ms": ms_per_step, "frac_of_bound": bound / t_meas,
-        "window_sample_bytes": n_lors * (rec + 4) + per * slots,
-        "window_sample_frac_hbm": (n_lors * (rec + 4) + per * slots) / (hbm_peak * 1e9) / t_meas,
+        "window_sample_bytes": lor_passes * n_lors * (rec + 4) + per * slots,
+        "window_sample_frac_hbm": (lor_passes * n_lors * (rec + 4) + per * slots)
+                                  / (hbm_peak * 1e9) / t_meas,
         "probe": probe["method"],
     }
 
@@ -335,7 +352,7 @@ def run_siddon(args):
     Siddon projection of all events, then the reference back-projection A^T(1/Ax). Also
     times one OSEM iteration (4 subsets, effmap from 10M random crystal pairs) and the
     reference's host-built Siddon pair on a bounded sample."""
-    from srf_b200 import CompleteLoRsModel, Image, backprojection, ops, profiling, projection
+    from srf_b200 import CompleteLoRsModel, Image, ops, profiling
     from srf_b200 import recon
     from srf_b200 import synthetic as S
     from srf_b200 import _lib
@@ -359,8 +376,7 @@ def run_siddon(args):
     visits = int(ops.siddon_count_samples(events, g, c, sz, layout="nc").sum(dtype=torch.int64))
 
     def step():
-        p = projection(model, image, data)
-        bp = backprojection(model, p, image)
+        bp = project_back(model, image, data, args.combined)
         if world > 1:
             import torch.distributed as dist
             dist.all_reduce(bp.data)
@@ -396,7 +412,7 @@ def run_siddon(args):
 
         def compute(ev):
             d = ListModeData(ev, torch.ones(ev.shape[0], device=dev))
-            bp = backprojection(model, projection(model, image, d), image)
+            bp = project_back(model, image, d, args.combined)
             if world > 1:
                 import torch.distributed as dist
                 dist.all_reduce(bp.data)
@@ -763,7 +779,7 @@ def main(argv=None):
 
     world, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
-    from srf_b200 import Image, backprojection, projection, profiling
+    from srf_b200 import Image, profiling
     from srf_b200 import preprocess as PP
 
     if args.tuning:
@@ -783,8 +799,7 @@ def main(argv=None):
     work = algorithmic_work(model, data, image)
 
     def step():
-        p = projection(model, image, data)
-        bp = backprojection(model, p, image)
+        bp = project_back(model, image, data, args.combined)
         if world > 1:
             import torch.distributed as dist
             dist.all_reduce(bp.data)
@@ -833,8 +848,7 @@ def main(argv=None):
             if args.order:
                 g = PP.order_by_direction(g)
             d = PP.split_listmode(g)
-            p = projection(model, image, d)
-            bp = backprojection(model, p, image)
+            bp = project_back(model, image, d, args.combined)
             if world > 1:
                 import torch.distributed as dist
                 dist.all_reduce(bp.data)
@@ -884,6 +898,10 @@ def main(argv=None):
     rec = 40  # bytes of one preprocessed LOR record (10 float32)
     alg = {"srf_tor_projection": n_lors * (rec + 4) + 4 * useful,
            "srf_tor_backprojection": n_lors * (rec + 4) + 8 * useful}
+    # the combined call runs both ops: each reads the records once, the values pass
+    # through HBM once each way, and every useful sample is read then read-modify-written
+    alg["srf_tor_projection_backprojection"] = (alg["srf_tor_projection"]
+                                                + alg["srf_tor_backprojection"])
     roof = None
     peaks_probe = profiling.measure_peaks() if kern else None
     if kern:

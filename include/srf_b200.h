@@ -78,6 +78,20 @@ int srf_tor_backprojection(const float *x1, const float *y1, const float *z1, co
                            float tof_sigma2, float *image, int64_t num_events,
                            int64_t lor_stride, int accumulate, void *stream);
 
+/* The reference's projection followed by its back-projection of the result, in one call
+ * (the numerator of the reference's recon step, model/recon_step.py:38-40, done there as
+ * two op calls): projection_value = A image (as srf_tor_projection) and
+ * back_image = A^T(1 / projection_value) with the 1e-7 threshold (as
+ * srf_tor_backprojection, `accumulate` likewise). No counterpart as one call in the
+ * reference: both ops share one set of per-slab LOR lists. back_image must not alias image. */
+int srf_tor_projection_backprojection(
+    const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
+    const float *z2, const float *xc, const float *yc, const float *zc,
+    const float *sigma2_factor, int geo_sigma2_flag, float *projection_value, const int *grid,
+    const float *center, const float *size, float kernel_width, float tof_bin, float tof_sigma2,
+    const float *image, float *back_image, int64_t num_events, int64_t lor_stride,
+    int accumulate, void *stream);
+
 /* Replaces maplors(), tor.cu.cc:435-481 (TF op "Maplors", tor.cc:49-64): geometric
  * weight only (no TOF), image += weight / projection_value[i] with no threshold. */
 int srf_tor_maplors(const float *x1, const float *y1, const float *z1, const float *x2,

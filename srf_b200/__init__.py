@@ -18,7 +18,7 @@ from . import data, ops, physics, preprocess  # noqa: F401
 from .data import (Image, ListModeData, ListModeDataSplit, ListModeDataSplitWithoutTOF,  # noqa
                    ListModeDataWithoutTOF)
 from .physics import (CompleteLoRsModel, SplitLoRsModel, backproject_adjoint,  # noqa: F401
-                      backprojection, map_lors, projection)
+                      backprojection, map_lors, projection, projection_backprojection)
 from .preprocess import map_process, recon_process  # noqa: F401
 
 __version__ = "0.1.0"

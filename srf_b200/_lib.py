@@ -29,6 +29,8 @@ SIGNATURES = {
                            _int),
     "srf_tor_backprojection": (_TOR_COLS + [_int, _p, _p, _p, _p, _f, _f, _f, _p, _i64, _i64,
                                             _int, _p], _int),
+    "srf_tor_projection_backprojection": (_TOR_COLS + [_int, _p, _p, _p, _p, _f, _f, _f, _p, _p,
+                                                   _i64, _i64, _int, _p], _int),
     "srf_tor_maplors": ([_p] * 7 + [_int, _p, _p, _p, _p, _f, _p, _i64, _i64, _int, _p], _int),
     "srf_tor_backproject_adjoint": (_TOR_COLS + [_int, _p, _p, _p, _p, _f, _f, _f, _p, _i64,
                                                  _i64, _int, _p], _int),

@@ -1074,8 +1074,35 @@ TorParams lor_chunk(const TorParams &p, int64_t c0, int64_t n) {
     return q;
 }
 
+// The slab kernel instance for p's variant, with its shared-memory limit raised once per
+// device.
 template <int OP, int P>
-int launch_slab(const TorParams &p, cudaStream_t stream) {
+int slab_kernel(const TorParams &p, bool band, void (**kern)(const TorParams, SegPlan)) {
+    *kern = p.slab_expand
+                ? (band ? tor_slab_kernel<OP, P, true, true> : tor_slab_kernel<OP, P, true, false>)
+                : (band ? tor_slab_kernel<OP, P, false, true> : tor_slab_kernel<OP, P, false, false>);
+    static std::atomic<unsigned long long> attr_set[4];  // per kernel instance, per device
+    std::atomic<unsigned long long> &done = attr_set[(p.slab_expand ? 2 : 0) + (band ? 1 : 0)];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+    if (!(done.load() & (1ull << dev))) {
+        const cudaError_t e = cudaFuncSetAttribute(
+            *kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmemBytes);
+        if (e != cudaSuccess) {
+            set_cuda_error(e);
+            return SRF_ERR_CUDA;
+        }
+        done.fetch_or(1ull << dev);
+    }
+    return SRF_OK;
+}
+
+// One TOR op over the slab path; with OP2 >= 0 a second op (p2: the same LORs and
+// geometry) runs on the same per-slab LOR lists right after the first, chunk by chunk
+// (the projection's lists serve the back-projection: it drops LORs below its value
+// threshold itself). Returns -1 when the slab path does not apply.
+template <int OP, int P, int OP2>
+int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
     SegPlan sp{};
     if (!slab_geometry(p, P - 1, sp)) return -1;
     // The segment list is sized for the worst case (every LOR in every slab of its frame);
@@ -1109,22 +1136,15 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
     sp.seg = reinterpret_cast<int *>(ws + b_range + b_counts + b_offs + b_slab);
 
     const bool band = sp.nbands > 1;
-    void (*kern)(const TorParams, SegPlan) =
-        p.slab_expand ? (band ? tor_slab_kernel<OP, P, true, true> : tor_slab_kernel<OP, P, true, false>)
-                      : (band ? tor_slab_kernel<OP, P, false, true> : tor_slab_kernel<OP, P, false, false>);
-    static std::atomic<unsigned long long> attr_set[4];  // per kernel instance, per device
-    std::atomic<unsigned long long> &done = attr_set[(p.slab_expand ? 2 : 0) + (band ? 1 : 0)];
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
-    if (!(done.load() & (1ull << dev))) {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSlabSmemBytes);
-        if (e != cudaSuccess) {
-            set_cuda_error(e);
-            cudaFreeAsync(ws, stream);
-            return SRF_ERR_CUDA;
-        }
-        done.fetch_or(1ull << dev);
+    void (*kern)(const TorParams, SegPlan) = nullptr;
+    void (*kern2)(const TorParams, SegPlan) = nullptr;
+    int st = slab_kernel<OP, P>(p, band, &kern);
+    if constexpr (OP2 >= 0) {
+        if (st == SRF_OK) st = slab_kernel<OP2, P>(*p2, band, &kern2);
+    }
+    if (st != SRF_OK) {
+        cudaFreeAsync(ws, stream);
+        return st;
     }
     const size_t smem = sizeof(float) * (size_t)slab_floats(sp.nsl, p.gx, sp.band_rows, P - 1);
     int64_t *slab_tot = sp.slab_offs + sp.n_slabs + 1;
@@ -1138,7 +1158,6 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
     }
     const int mult = std::max(1, std::min(8, g_tune_mult.load(std::memory_order_relaxed)));
     const size_t hist_bytes = sizeof(int) * (size_t)sp.n_slabs;  // <= 16 KB (kMaxSlabs)
-    int st = SRF_OK;
     for (int64_t c0 = 0; c0 < p.n && st == SRF_OK; c0 += chunk) {
         const TorParams q = lor_chunk(p, c0, std::min(chunk, p.n - c0));
         SegPlan sq = sp;
@@ -1155,6 +1174,11 @@ int launch_slab(const TorParams &p, cudaStream_t stream) {
             seg_fill_kernel<false><<<sq.ntiles, kSegThreads, hist_bytes, stream>>>(q, sq);
         kern<<<num_sms() * mult, kSlabThreads, smem, stream>>>(q, sq);
         count_launches(5);
+        if constexpr (OP2 >= 0) {
+            kern2<<<num_sms() * mult, kSlabThreads, smem, stream>>>(
+                lor_chunk(*p2, c0, std::min(chunk, p.n - c0)), sq);
+            count_launches(1);
+        }
         st = check_launch();
     }
     e = cudaFreeAsync(ws, stream);
@@ -1171,13 +1195,13 @@ int tor_launch(TorParams &p, cudaStream_t stream, bool generic = false) {
     if ((OP == kProj || OP == kBack || OP == kMap || OP == kAdj) && !generic && p.use_slab) {
         int st = -1;
         switch (p.patch) {
-            case 2: st = launch_slab<OP, 2>(p, stream); break;
-            case 3: st = launch_slab<OP, 3>(p, stream); break;
-            case 4: st = launch_slab<OP, 4>(p, stream); break;
-            case 5: st = launch_slab<OP, 5>(p, stream); break;
-            case 6: st = launch_slab<OP, 6>(p, stream); break;
-            case 7: st = launch_slab<OP, 7>(p, stream); break;
-            case 8: st = launch_slab<OP, 8>(p, stream); break;
+            case 2: st = launch_slab<OP, 2, -1>(p, nullptr, stream); break;
+            case 3: st = launch_slab<OP, 3, -1>(p, nullptr, stream); break;
+            case 4: st = launch_slab<OP, 4, -1>(p, nullptr, stream); break;
+            case 5: st = launch_slab<OP, 5, -1>(p, nullptr, stream); break;
+            case 6: st = launch_slab<OP, 6, -1>(p, nullptr, stream); break;
+            case 7: st = launch_slab<OP, 7, -1>(p, nullptr, stream); break;
+            case 8: st = launch_slab<OP, 8, -1>(p, nullptr, stream); break;
             default: break;
         }
         if (st >= 0) return st;
@@ -1198,6 +1222,28 @@ int tor_launch(TorParams &p, cudaStream_t stream, bool generic = false) {
             break;
     }
     return check_launch();
+}
+
+// Projection pp then back-projection pb of its values (same LORs, geometry and tuning):
+// on the slab path both ops share one set of per-slab LOR lists.
+int tor_launch_pair(TorParams &pp, TorParams &pb, cudaStream_t stream) {
+    if (pp.n == 0) return SRF_OK;
+    int st = -1;
+    if (pp.use_slab) {
+        switch (pp.patch) {
+            case 2: st = launch_slab<kProj, 2, kBack>(pp, &pb, stream); break;
+            case 3: st = launch_slab<kProj, 3, kBack>(pp, &pb, stream); break;
+            case 4: st = launch_slab<kProj, 4, kBack>(pp, &pb, stream); break;
+            case 5: st = launch_slab<kProj, 5, kBack>(pp, &pb, stream); break;
+            case 6: st = launch_slab<kProj, 6, kBack>(pp, &pb, stream); break;
+            case 7: st = launch_slab<kProj, 7, kBack>(pp, &pb, stream); break;
+            case 8: st = launch_slab<kProj, 8, kBack>(pp, &pb, stream); break;
+            default: break;
+        }
+    }
+    if (st >= 0) return st;
+    st = tor_launch<kProj>(pp, stream);
+    return st == SRF_OK ? tor_launch<kBack>(pb, stream) : st;
 }
 
 int zero_image(float *image, const int *grid, cudaStream_t stream) {
@@ -1270,6 +1316,35 @@ extern "C" int srf_tor_backprojection(const float *x1, const float *y1, const fl
     p.values = projection_value;
     p.image_out = image;
     return tor_launch<kBack>(p, (cudaStream_t)stream);
+}
+
+extern "C" int srf_tor_projection_backprojection(
+    const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
+    const float *z2, const float *xc, const float *yc, const float *zc,
+    const float *sigma2_factor, int geo_sigma2_flag, float *projection_value, const int *grid,
+    const float *center, const float *size, float kernel_width, float tof_bin, float tof_sigma2,
+    const float *image, float *back_image, int64_t num_events, int64_t lor_stride,
+    int accumulate, void *stream) {
+    TorParams pp{};
+    int st = tor_setup(pp, grid, center, size, kernel_width, tof_bin, tof_sigma2, num_events,
+                       lor_stride);
+    if (st != SRF_OK) return st;
+    if (!back_image || back_image == image) return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > 0 &&
+        !cols_ok({x1, y1, z1, x2, y2, z2, sigma2_factor, projection_value, image}))
+        return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > 0 && pp.tof_on && !cols_ok({xc, yc, zc})) return SRF_ERR_INVALID_ARGUMENT;
+    if (!accumulate && (st = zero_image(back_image, grid, (cudaStream_t)stream)) != SRF_OK)
+        return st;
+    pp.x1 = x1; pp.y1 = y1; pp.z1 = z1; pp.x2 = x2; pp.y2 = y2; pp.z2 = z2;
+    pp.xc = xc; pp.yc = yc; pp.zc = zc; pp.f = sigma2_factor;
+    pp.geo = geo_sigma2_flag != 0;
+    TorParams pb = pp;
+    pp.image_in = image;
+    pp.proj_out = projection_value;
+    pb.values = projection_value;
+    pb.image_out = back_image;
+    return tor_launch_pair(pp, pb, (cudaStream_t)stream);
 }
 
 extern "C" int srf_tor_maplors(const float *x1, const float *y1, const float *z1,

@@ -171,6 +171,30 @@ def tor_backprojection(image, lors, lors_value, grid, center, size, kernel_width
                         accumulate)
 
 
+def tor_projection_backprojection(lors, image, grid, center, size, kernel_width,
+                                  geo_sigma2_flag=False, tof_bin=1.0e4, tof_sigma2=1.0e4,
+                                  layout="auto", out_values=None, out=None, accumulate=False):
+    """``tor_projection`` then ``tor_backprojection`` of its values in one call (both
+    kernels share one set of per-slab LOR lists). Returns (values, back image)."""
+    dev = _check_cuda(lors, image, out_values, out)
+    t, cols, n, stride = _columns(lors, TOR_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    img = _as_image(image, g)
+    if out_values is None:
+        out_values = torch.empty(n, dtype=torch.float32, device=dev)
+    elif out_values.numel() != n or not out_values.is_contiguous():
+        raise ValueError("out_values must be a contiguous tensor with one entry per LOR")
+    res, _ = _out_image(out, g, lors)
+    if res.data_ptr() == img.data_ptr():
+        raise ValueError("the back-projection must not overwrite the projected image")
+    with torch.cuda.device(dev):
+        _call(dev, "srf_tor_projection_backprojection", *cols[:10], int(bool(geo_sigma2_flag)),
+              out_values.data_ptr(), ga, ca, sa, float(kernel_width), float(tof_bin),
+              float(tof_sigma2), img.data_ptr(), res.data_ptr(), n, stride,
+              int(bool(accumulate) and out is not None), _stream(dev))
+    return out_values, res
+
+
 def tor_backproject_adjoint(values, lors, grid, center, size, kernel_width,
                             geo_sigma2_flag=False, tof_bin=1.0e4, tof_sigma2=1.0e4,
                             layout="auto", out=None, accumulate=False):

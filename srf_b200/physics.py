@@ -193,6 +193,28 @@ def backprojection(model, data, image):
     raise TypeError(f"no backprojection for {type(model).__name__}")
 
 
+def projection_backprojection(model, image, data):
+    """``backprojection(model, projection(model, image, data), image)`` with the projected
+    data too; for TOR each axis group is one combined library call. Returns
+    (projected list-mode data, back-projected ``Image``)."""
+    if isinstance(model, SplitLoRsModel) and isinstance(data, ListModeDataSplit) \
+            and not isinstance(data, ListModeDataSplitWithoutTOF):
+        res, parts = {}, []
+        for a in model.AXIS:
+            if data[a].lors.shape[0] == 0:
+                res[a] = torch.zeros(0, dtype=torch.float32, device=data[a].lors.device)
+                continue
+            img, g, c, s = model.kernel_geometry(image, a)
+            res[a], bp = ops.tor_projection_backprojection(
+                _lors_of(data[a]), img, g, c, s, model.kernel_width, model.geo_sigma2_flag,
+                model.tof_bin, model.tof_sigma2, layout="nc")
+            parts.append((a, bp))
+        proj = ListModeDataSplit(*[ListModeData(data[a].lors, res[a]) for a in model.AXIS])
+        return proj, _sum_back(model, parts, image)
+    proj = projection(model, image, data)
+    return proj, backprojection(model, proj, image)
+
+
 def backproject_adjoint(model, data, image):
     """The plain transpose Aᵀ·values (no division): autograd's backward and the
     textbook OSEM numerator."""

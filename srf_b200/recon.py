@@ -29,7 +29,7 @@ import torch
 
 from . import ops
 from .data import Image, ListModeData, ListModeDataSplit
-from .physics import CompleteLoRsModel, SplitLoRsModel, backprojection, map_lors, projection
+from .physics import CompleteLoRsModel, SplitLoRsModel, map_lors, projection_backprojection
 from .preprocess import crop_mask, map_process, merge_effmap, split_listmode
 
 
@@ -56,8 +56,7 @@ class ReconStep:
         self.update = update
 
     def __call__(self, image, efficiency_map, projection_data):
-        proj = projection(self.model, image, projection_data)
-        back = backprojection(self.model, proj, image)
+        _, back = projection_backprojection(self.model, image, projection_data)
         return self.update(image, back, efficiency_map)
 
 
@@ -159,8 +158,7 @@ class OSEM:
         self.iteration = 0
 
     def _subset_update(self, k):
-        proj = projection(self.model, self.x, self.subsets[k])
-        back = backprojection(self.model, proj, self.x)
+        _, back = projection_backprojection(self.model, self.x, self.subsets[k])
         ops.mlem_update_(self.x.data, self.effinv.data, back.data)
 
     def _iterate(self):

@@ -338,6 +338,8 @@ def test_empty_inputs():
     bp = host(ops.tor_backprojection(img, e10, torch.zeros(0, device="cuda"), g, c, s, 4.0,
                                      layout="cn"))
     assert bp.shape == (8, 16, 16) and not bp.any()
+    pv, bp = ops.tor_projection_backprojection(e10, img, g, c, s, 4.0, layout="cn")
+    assert pv.numel() == 0 and not host(bp).any()
     e7 = torch.zeros((7, 0), device="cuda")
     assert ops.siddon_projection(e7, img, g, c, s, layout="cn").numel() == 0
 
@@ -431,6 +433,60 @@ def test_slab_chunks_equal_one_pass():
         tuning.set_scratch_limit(1)
         try:
             chunked = run()
+        finally:
+            tuning.set_scratch_limit(0)
+    finally:
+        tuning.set_tuning()
+    for a, b_ in zip(one, chunked):
+        assert np.count_nonzero(a) > 0
+        assert K.rel_l2(b_, a) <= 1e-6
+
+
+@pytest.mark.parametrize("pname", ["tof530_kw10", "tof530_kw4_geo", "notof"])
+@pytest.mark.parametrize("axis", ["x", "y", "z"])
+def test_tor_projection_backprojection_combined(tcase, pname, axis, tor_path):
+    """The combined call gives the separate calls' projection values and back-projected
+    image in every kernel family, and both match the oracle."""
+    kw, geo, b, s2 = _tp(pname)
+    lors, img, g, c, s = K.tor_axis(tcase, axis)
+    L, I = cu(lors), cu(img)
+    pv_t, bp_t = ops.tor_projection_backprojection(L, I, g, c, s, kw, geo, b, s2, layout="cn")
+    pv, bp = host(pv_t), host(bp_t)
+    pv_sep = ops.tor_projection(L, I, g, c, s, kw, geo, b, s2, layout="cn")
+    bp_sep = host(ops.tor_backprojection(I, L, pv_sep, g, c, s, kw, geo, b, s2, layout="cn"))
+    assert K.rel_l2(pv, host(pv_sep)) <= 1e-6
+    assert K.rel_l2(bp, bp_sep) <= 1e-6
+    f32 = O.tor_projection(lors, img, g, c, s, kw, geo, b, s2, mode="f32", contract=True)
+    back = O.tor_backprojection(lors, f32, g, c, s, kw, geo, b, s2, mode="f32", contract=True)
+    e_p, e_b = K.rel_l2(pv, f32), K.rel_l2(bp, back)
+    record("tor_projection_backprojection", params=pname, axis=axis, rel_l2_proj=e_p,
+           rel_l2_back=e_b)
+    assert np.count_nonzero(back) > 0
+    assert e_p <= TOL and e_b <= TOL, (e_p, e_b)
+    # accumulate adds onto the given image; the image must not be overwritten in place
+    acc = cu(np.full(img.shape, 2.0, np.float32))
+    ops.tor_projection_backprojection(L, I, g, c, s, kw, geo, b, s2, layout="cn", out=acc,
+                                      accumulate=True)
+    assert K.rel_l2(host(acc), bp + 2.0) <= 1e-6
+    with pytest.raises(ValueError):
+        ops.tor_projection_backprojection(L, I, g, c, s, kw, geo, b, s2, layout="cn", out=I)
+
+
+def test_tor_projection_backprojection_chunked():
+    """With one 4096-LOR chunk at a time the combined call still equals one pass."""
+    from srf_b200 import tuning
+    big = K.tor_case(n=40000, seed=91, grid=(128, 128, 64), voxel=3.2, n_box=4000)
+    kw, geo, b, s2 = _tp("tof530_kw10")
+    lors, img, g, c, s = K.tor_axis(big, "x")
+    L, I = cu(lors), cu(img)
+    tuning.set_tuning(path=1)
+    try:
+        one = [host(t) for t in ops.tor_projection_backprojection(L, I, g, c, s, kw, geo, b, s2,
+                                                                  layout="cn")]
+        tuning.set_scratch_limit(1)
+        try:
+            chunked = [host(t) for t in ops.tor_projection_backprojection(
+                L, I, g, c, s, kw, geo, b, s2, layout="cn")]
         finally:
             tuning.set_scratch_limit(0)
     finally:
