@@ -213,17 +213,23 @@ __global__ void __launch_bounds__(1024) scan_kernel(const PreParams p) {
     }
 }
 
+// Per step of kThreads events: each event's rank inside its bucket (warp ballots in index
+// order), its record written to a shared staging buffer compacted by bucket, then each
+// bucket's run copied to its place in the output as one contiguous stretch (a record
+// is 28-40 bytes, so one thread per record would touch a new sector per lane and column).
 template <bool RECON>
 __global__ void __launch_bounds__(kThreads) scatter_kernel(const PreParams p) {
+    constexpr int ncols = RECON ? 10 : 7;
     __shared__ int warp_counts[kThreads / 32][kBuckets];
     __shared__ int64_t running[kBuckets];
+    __shared__ int step_start[kBuckets + 1];  // bucket runs in the staging buffer
+    __shared__ float stage[kThreads * ncols];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (threadIdx.x < kBuckets)
         running[threadIdx.x] =
             p.bucket_base[threadIdx.x] + p.tile_offsets[blockIdx.x * kBuckets + threadIdx.x];
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kTile;
-    constexpr int ncols = RECON ? 10 : 7;
     for (int k = 0; k < kItems; k++) {
         const int64_t i = base + (int64_t)k * kThreads + threadIdx.x;
         const int b = i < p.n ? (int)p.bucket[i] : kBuckets;
@@ -236,24 +242,33 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const PreParams p) {
             if (lane == 0) warp_counts[wid][q] = __popc(m);
         }
         __syncthreads();
-        int64_t dest = -1;
-        if (b < kBuckets) {
-            int64_t before = running[b];
-            for (int w = 0; w < wid; w++) before += warp_counts[w][b];
-            dest = before + my_rank;
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int q = 0; q < kBuckets; q++) {
+                step_start[q] = acc;
+                for (int w = 0; w < kThreads / 32; w++) acc += warp_counts[w][q];
+            }
+            step_start[kBuckets] = acc;
         }
         __syncthreads();
-        if (threadIdx.x < kBuckets) {
-            int64_t add = 0;
-            for (int w = 0; w < kThreads / 32; w++) add += warp_counts[w][threadIdx.x];
-            running[threadIdx.x] += add;
-        }
-        if (dest >= 0) {
+        if (b < kBuckets) {
+            int pos = step_start[b] + my_rank;
+            for (int w = 0; w < wid; w++) pos += warp_counts[w][b];
             const Rec r = process<RECON>(p.events + i * p.stride, p.cut, p.limit);
-            float *o = p.out + dest * ncols;
 #pragma unroll
-            for (int c = 0; c < ncols; c++) o[c] = r.v[c];
+            for (int c = 0; c < ncols; c++) stage[pos * ncols + c] = r.v[c];
         }
+        __syncthreads();
+        const int total = step_start[kBuckets] * ncols;
+        for (int e = threadIdx.x; e < total; e += kThreads) {
+            const int rec = e / ncols;
+            int q = 0;
+            while (rec >= step_start[q + 1]) q++;
+            p.out[(running[q] + (rec - step_start[q])) * ncols + (e - rec * ncols)] = stage[e];
+        }
+        __syncthreads();
+        if (threadIdx.x < kBuckets)
+            running[threadIdx.x] += step_start[threadIdx.x + 1] - step_start[threadIdx.x];
         __syncthreads();
     }
 }

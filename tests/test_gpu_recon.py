@@ -368,6 +368,37 @@ def test_order_by_direction_permutes_within_blocks_and_keeps_the_reconstruction(
     assert float((bp[1] - bp[0]).norm() / bp[0].norm()) < 1e-6
 
 
+def test_order_by_direction_staged_equals_per_record():
+    """Records of up to 10 columns are reordered through shared memory, wider ones one
+    thread per record; both give the same order (checked bit for bit on the same records,
+    contiguous and with a record stride wider than the record)."""
+    from srf_b200 import _lib
+    ev = K.events(30_000, 23, 530.0).astype(np.float32)
+    g = _recon_groups(ev)["x"]
+    n = g.shape[0]
+    wide = torch.cat([g, torch.arange(2 * n, device="cuda", dtype=torch.float32).view(n, 2)],
+                     1).contiguous()  # 12 columns: the per-record kernel
+    out_wide = torch.empty_like(wide)
+    _lib.call("srf_order_by_direction", wide.data_ptr(), n, 12, 12, out_wide.data_ptr(), None)
+    narrow = g.contiguous()
+    out_narrow = torch.empty_like(narrow)
+    _lib.call("srf_order_by_direction", narrow.data_ptr(), n, 10, 10, out_narrow.data_ptr(),
+              None)
+    out_strided = torch.zeros_like(wide)  # 10 columns read and written at a 12-float stride
+    _lib.call("srf_order_by_direction", wide.data_ptr(), n, 10, 12, out_strided.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert n > 3 * 4096
+    assert torch.equal(out_wide[:, :10], out_narrow)
+    assert torch.equal(out_strided[:, :10], out_narrow)
+    assert not out_strided[:, 10:].any()  # columns past ncols are left alone
+    assert not torch.equal(out_narrow, narrow)  # the order did change
+
+
+def _recon_groups(ev):
+    from srf_b200 import preprocess as PP
+    return PP.recon_process(cu(ev), 530.0)
+
+
 def test_siddon_osem_ordered_equals_unordered():
     """Ray ordering by walk length changes the summation order only."""
     from srf_b200 import CompleteLoRsModel
