@@ -122,6 +122,18 @@ int srf_tor_count_samples(const float *x1, const float *y1, const float *z1, con
                           const float *size, float kernel_width, int *counts,
                           int64_t num_events, int64_t lor_stride, void *stream);
 
+/* srf_tor_projection_backprojection for batched frames (frame, n_frames, frame_stride as
+ * in srf_tor_projection_batched): projection_value from the frames' images, then
+ * back_images (same layout, must not alias images) += A^T(1 / projection_value) per frame.
+ * No counterpart in the reference. */
+int srf_tor_projection_backprojection_batched(
+    const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
+    const float *z2, const float *xc, const float *yc, const float *zc,
+    const float *sigma2_factor, int geo_sigma2_flag, const int *frame, int n_frames,
+    int64_t frame_stride, float *projection_value, const int *grid, const float *center,
+    const float *size, float kernel_width, float tof_bin, float tof_sigma2, const float *images,
+    float *back_images, int64_t num_events, int64_t lor_stride, int accumulate, void *stream);
+
 /* No counterpart in the reference: batched TOR for many reconstructions that share one
  * geometry (dynamic frames, many phantoms). LOR i belongs to frame frame[i] (DEVICE
  * int32[N], 0 <= frame[i] < n_frames); images are n_frames consecutive blocks of

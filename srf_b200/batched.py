@@ -7,8 +7,8 @@ Per frame the arithmetic is exactly ``srf_b200.recon.OSEM``'s (the same subsets,
 same reference back-projection A^T(1/Ax), the same update); what changes is the launch
 structure: the LORs of every frame are concatenated per dominant axis with a frame
 index, the images are stacked [F, nx, ny, nz], and each subset is one batched
-projection and one batched back-projection per axis group for ALL frames — one
-persistent launch per kernel instead of one per frame, with the work balanced across
+projection and back-projection call per axis group for ALL frames — one persistent
+launch per kernel instead of one per frame, with the work balanced across
 SMs over the frames' combined segments. An iteration can be captured in a CUDA graph.
 """
 
@@ -95,12 +95,9 @@ class BatchedOSEM:
             if lors.shape[0] == 0:
                 continue
             img_a = self.x.permute(*_stacked_perm(m.perm(a))).contiguous()
-            pv = ops.tor_projection_batched(lors, frame, img_a, self.F, g, c, s, m.kernel_width,
-                                            m.geo_sigma2_flag, m.tof_bin, m.tof_sigma2,
-                                            layout="nc")
-            bk = ops.tor_backprojection_batched(lors, frame, pv, self.F, g, c, s,
-                                                m.kernel_width, m.geo_sigma2_flag, m.tof_bin,
-                                                m.tof_sigma2, layout="nc")
+            _, bk = ops.tor_projection_backprojection_batched(
+                lors, frame, img_a, self.F, g, c, s, m.kernel_width, m.geo_sigma2_flag,
+                m.tof_bin, m.tof_sigma2, layout="nc")
             back = bk.permute(*_stacked_perm(m.perm_back(a)))
             bp = back.clone() if bp is None else bp.add_(back)
         if bp is None:

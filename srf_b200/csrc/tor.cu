@@ -1511,6 +1511,37 @@ extern "C" int srf_tor_backprojection_batched(
                                   stream);
 }
 
+extern "C" int srf_tor_projection_backprojection_batched(
+    const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
+    const float *z2, const float *xc, const float *yc, const float *zc,
+    const float *sigma2_factor, int geo_sigma2_flag, const int *frame, int n_frames,
+    int64_t frame_stride, float *projection_value, const int *grid, const float *center,
+    const float *size, float kernel_width, float tof_bin, float tof_sigma2, const float *images,
+    float *back_images, int64_t num_events, int64_t lor_stride, int accumulate, void *stream) {
+    TorParams pp{};
+    int st = tor_setup(pp, grid, center, size, kernel_width, tof_bin, tof_sigma2, num_events,
+                       lor_stride);
+    if (st != SRF_OK) return st;
+    if ((st = set_frames(pp, frame, n_frames, frame_stride)) != SRF_OK) return st;
+    if (!back_images || back_images == images) return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > 0 &&
+        !cols_ok({x1, y1, z1, x2, y2, z2, sigma2_factor, projection_value, images}))
+        return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > 0 && pp.tof_on && !cols_ok({xc, yc, zc})) return SRF_ERR_INVALID_ARGUMENT;
+    if (!accumulate &&
+        (st = zero_frames(back_images, n_frames, frame_stride, (cudaStream_t)stream)) != SRF_OK)
+        return st;
+    pp.x1 = x1; pp.y1 = y1; pp.z1 = z1; pp.x2 = x2; pp.y2 = y2; pp.z2 = z2;
+    pp.xc = xc; pp.yc = yc; pp.zc = zc; pp.f = sigma2_factor;
+    pp.geo = geo_sigma2_flag != 0;
+    TorParams pb = pp;
+    pp.image_in = images;
+    pp.proj_out = projection_value;
+    pb.values = projection_value;
+    pb.image_out = back_images;
+    return tor_launch_pair(pp, pb, (cudaStream_t)stream);
+}
+
 extern "C" int srf_tor_backproject_adjoint_batched(
     const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
     const float *z2, const float *xc, const float *yc, const float *zc,

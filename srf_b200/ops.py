@@ -356,6 +356,39 @@ def tor_projection_batched(lors, frame, images, n_frames, grid, center, size, ke
     return out
 
 
+def tor_projection_backprojection_batched(lors, frame, images, n_frames, grid, center, size,
+                                          kernel_width, geo_sigma2_flag=False, tof_bin=1.0e4,
+                                          tof_sigma2=1.0e4, layout="auto", out_values=None,
+                                          out=None, accumulate=False):
+    """``tor_projection_batched`` then ``tor_backprojection_batched`` of its values in one
+    call (one set of per-slab LOR lists for both). Returns (values, back images)."""
+    dev = _check_cuda(lors, images, out_values, out)
+    t, cols, n, stride = _columns(lors, TOR_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    fr, nvox = _frame_args(frame, n_frames, images.numel(), g)
+    if fr.numel() != n:
+        raise ValueError("frame needs one entry per LOR")
+    imgs = images.contiguous()
+    if out_values is None:
+        out_values = torch.empty(n, dtype=torch.float32, device=dev)
+    elif out_values.numel() != n or not out_values.is_contiguous():
+        raise ValueError("out_values must be a contiguous tensor with one entry per LOR")
+    if out is None:
+        out = torch.empty((n_frames, g[2], g[1], g[0]), dtype=torch.float32, device=dev)
+        accumulate = False
+    elif out.numel() != n_frames * nvox or not out.is_contiguous():
+        raise ValueError("out must be a contiguous stack of n_frames images")
+    if out.data_ptr() == imgs.data_ptr():
+        raise ValueError("the back-projection must not overwrite the projected images")
+    with torch.cuda.device(dev):
+        _call(dev, "srf_tor_projection_backprojection_batched", *cols[:10],
+              int(bool(geo_sigma2_flag)), fr.data_ptr(), int(n_frames), nvox,
+              out_values.data_ptr(), ga, ca, sa, float(kernel_width), float(tof_bin),
+              float(tof_sigma2), imgs.data_ptr(), out.data_ptr(), n, stride,
+              int(bool(accumulate)), _stream(dev))
+    return out_values, out
+
+
 def _tor_scatter_batched(fn, lors, frame, values, n_frames, grid, center, size, kernel_width,
                          geo_sigma2_flag, tof_bin, tof_sigma2, layout, out, accumulate):
     dev = _check_cuda(lors, values, out)

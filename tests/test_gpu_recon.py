@@ -177,6 +177,11 @@ def test_batched_ops_equal_per_frame(tune):
                                              K.KW_CONFIG, False, b, s2, layout="nc")
                 assert K.rel_l2(bp[i].cpu().numpy(), one.cpu().numpy()) < 1e-6
                 off += n
+            # the combined batched call gives both results at once
+            pv2, bp2 = ops.tor_projection_backprojection_batched(
+                lors, frame, stack, len(frames), g, c, s, K.KW_CONFIG, False, b, s2, layout="nc")
+            assert K.rel_l2(pv2.cpu().numpy(), pv.cpu().numpy()) < 1e-6
+            assert K.rel_l2(bp2.cpu().numpy(), bp.cpu().numpy()) < 1e-6
     finally:
         tuning.set_tuning()
 
