@@ -70,10 +70,13 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--workload", default="tor128",
-                    choices=["tor128", "large256", "siddon64", "batched96", "autograd128"],
+                    choices=["tor128", "large256", "large256_recon", "siddon64", "batched96",
+                             "autograd128"],
                     help="tor128: the headline TOF-TOR pair (default); large256: the same "
                          "pair on one 16M-event chunk of the large axial FOV workload "
-                         "(256x256x128 at 2.5 mm, 1 m axial, 400 ps); siddon64: the plain "
+                         "(256x256x128 at 2.5 mm, 1 m axial, 400 ps); large256_recon: that "
+                         "reconstruction end to end (200M events streamed in 16M chunks, "
+                         "effmap from 500M LORs, OSEM 2 x 20); siddon64: the plain "
                          "non-TOF Siddon pair and OSEM iteration (64x64x32, 1M events); "
                          "autograd128: forward + backward of 5 unrolled OSEM iterations "
                          "(128x128x64, 8 frames x 5M events); batched96: 64-frame "
@@ -100,6 +103,126 @@ def project_back(model, image, data, combined=True):
     if combined:
         return projection_backprojection(model, image, data)[1]
     return backprojection(model, projection(model, image, data), image)
+
+
+def time_osem(model, data, effinv, wl, dev, warmup=1):
+    """The workload's OSEM (wl.iterations x wl.subsets, records ordered inside each subset,
+    eager launches) timed with CUDA events after ``warmup`` untimed iterations of another
+    instance."""
+    from srf_b200 import recon
+    from srf_b200.preprocess import initial_image
+    x0 = _image_of(initial_image(list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
+                                wl.scanner.axial_length, dev), wl)
+    if warmup:
+        recon.OSEM(model, data, effinv, x0, n_subsets=wl.subsets).run(warmup)
+    osem = recon.OSEM(model, data, effinv, x0, n_subsets=wl.subsets)
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    osem.run(wl.iterations)
+    s1.record()
+    torch.cuda.synchronize()
+    ms = s0.elapsed_time(s1)
+    n = sum(data[a].lors.shape[0] for a in "xyz")
+    return {"iterations": wl.iterations, "subsets": wl.subsets, "ms": ms,
+            "ms_per_iteration": ms / wl.iterations,
+            "lors_per_s": n * wl.iterations / (ms / 1e3),
+            "path": "recon.OSEM: per subset one combined projection + back-projection call "
+                    "per axis group, then the multiplicative update"}
+
+
+def _image_of(t, wl):
+    from srf_b200 import Image
+    return Image(t, wl.center, wl.size)
+
+
+def run_large_recon(args):
+    """The large axial FOV reconstruction end to end: 200M seeded TOF events (400 ps) from
+    the multi-cylinder phantom, streamed in 16M-event chunks from pinned host memory
+    through recon_process; the efficiency map from 500M random detector pairs generated on
+    the device; OSEM 2 iterations x 20 subsets at 256x256x128 (2.5 mm). Each chunk's events
+    are generated on the device and copied to the pinned buffer outside the timed parts,
+    standing in for a read from storage."""
+    from srf_b200 import recon
+    from srf_b200 import preprocess as PP
+    from srf_b200 import synthetic as S
+    from srf_b200.preprocess import initial_image
+    from srf_b200.scanner import tof_info
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    wl = S.large_256()
+    n_total = args.events or wl.n_events
+    chunk = 16_000_000
+    tof_bin, tof_sigma2 = tof_info(wl.tof_res_ps, wl.tof_bin_ps)
+    model = model_for(wl, tof_bin, tof_sigma2)
+    phantom = S.large_fov_phantom(half_length=wl.scanner.axial_length / 2)
+    host = torch.empty((min(chunk, n_total), 7), dtype=torch.float32).pin_memory()
+    dbuf = torch.empty((min(chunk, n_total), 7), dtype=torch.float32, device=dev)
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        r = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(b)
+
+    parts, stream_ms, gen_s = {a: [] for a in "xyz"}, 0.0, 0.0
+    for k, start in enumerate(range(0, n_total, chunk)):
+        c = min(chunk, n_total - start)
+        t0 = time.perf_counter()
+        ev = S.generate_events(c, wl.scanner, phantom, seed=wl.seed * 1000 + k,
+                               tof_sigma_mm=math.sqrt(tof_sigma2), device=dev)
+        host[:c].copy_(ev)
+        del ev
+        gen_s += time.perf_counter() - t0
+
+        def upload_and_preprocess():
+            dbuf[:c].copy_(host[:c], non_blocking=True)
+            return PP.recon_process(dbuf[:c], wl.tof_res_ps)
+
+        g, ms = timed(upload_and_preprocess)
+        stream_ms += ms
+        for a in "xyz":
+            parts[a].append(g[a])
+    groups = {a: torch.cat(v) for a, v in parts.items()}
+    del parts
+    data = PP.split_listmode(groups)
+    args_e = (list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
+              wl.scanner.axial_length)
+    recon.efficiency_map(model, S.RandomLorSource(chunk, wl.scanner, 78, device=dev),
+                         *args_e)  # warm-up: one chunk (sizes the scratch pool)
+    (effinv, _), effmap_ms = timed(lambda: recon.efficiency_map(
+        model, S.RandomLorSource(wl.n_effmap, wl.scanner, 77, device=dev), *args_e))
+    x0 = _image_of(initial_image(list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
+                                 wl.scanner.axial_length, dev), wl)
+    osem, setup_ms = timed(lambda: recon.OSEM(model, data, effinv, x0, n_subsets=wl.subsets))
+    del data, groups
+    _, osem_ms = timed(lambda: osem.run(wl.iterations))
+    total_ms = stream_ms + effmap_ms + setup_ms + osem_ms
+    x = osem.x.data
+    line = {"metric": "large axial FOV TOF OSEM end to end (256x256x128, 200M events in "
+                      "16M-event chunks, 2 it x 20 subsets, effmap from 500M random LORs)",
+            "value": total_ms / 1e3, "unit": "s", "higher_is_better": False, "n_gpus": 1,
+            "events": n_total, "stream_preprocess_ms": stream_ms, "effmap_ms": effmap_ms,
+            "osem_setup_ms": setup_ms, "osem_ms": osem_ms,
+            "osem_lors_per_s": n_total * wl.iterations / (osem_ms / 1e3),
+            "effmap_lors_per_s": wl.n_effmap / (effmap_ms / 1e3),
+            "image_finite": bool(torch.isfinite(x).all()), "image_sum": float(x.sum()),
+            "generation_s_untimed": gen_s, "dtype": "f32",
+            "data": "synthetic (seeded events from the multi-cylinder phantom)",
+            "config": {"workload": "large_256x256x128_200M_recon", "grid": list(wl.grid),
+                       "voxel_mm": wl.voxel, "tof_res_ps": wl.tof_res_ps,
+                       "kernel_width": round(wl.kernel_width, 4), "chunk_events": chunk,
+                       "iterations": wl.iterations, "subsets": wl.subsets,
+                       "effmap_lors": wl.n_effmap},
+            "path": "per chunk: pinned host events -> device -> recon_process; effmap: "
+                    "on-device random pairs -> map_process -> maplors; OSEM: subsets split "
+                    "and ordered once, then per subset one combined projection + "
+                    "back-projection call per axis group and the update"}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 # ------------------------------------------------------------------ distributed
@@ -776,6 +899,8 @@ def main(argv=None):
         return run_siddon(args)
     if args.workload == "autograd128":
         return run_autograd(args)
+    if args.workload == "large256_recon":
+        return run_large_recon(args)
 
     world, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
@@ -876,7 +1001,7 @@ def main(argv=None):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        recon.efficiency_map(model, src, *args_e)
+        effinv, _ = recon.efficiency_map(model, src, *args_e)
         e1.record()
         torch.cuda.synchronize()
         e_ms = max_over_ranks(e0.elapsed_time(e1), world)
@@ -885,6 +1010,8 @@ def main(argv=None):
                   "path": "random crystal pairs generated on the device per chunk -> "
                           "map_process -> TOR maplors of each axis group -> crop, normalise, "
                           "invert"}
+        if wl.name == "tor_tof_128x128x64_10M" and world == 1:
+            effmap["osem"] = time_osem(model, data, effinv, wl, dev)
 
     # ---------------------------------------------------------------- roofline
     peaks = {}
