@@ -71,10 +71,12 @@ def split_listmode(groups, values=None, without_tof=False):
 # ------------------------------------------------------------------- effmap merge
 
 
-def crop_mask(grid, center, size, inner_radius, axial_length, crop_ratio=0.95):
+def crop_mask(grid, center, size, inner_radius, axial_length, crop_ratio=0.95, device=None):
     """Keep-mask of ``crop_image`` (merge_map.py:47-65) over the [nx,ny,nz] image. The
     reference pairs the mesh list of ``RingBlock.get_meshes`` (np.meshgrid 'xy' order:
-    iy, ix, iz) with the image flattened as (ix, iy, iz); the mask keeps that pairing."""
+    iy, ix, iz) with the image flattened as (ix, iy, iz); the mask keeps that pairing.
+    With ``device`` the mask is built there as a torch bool tensor (the same float64
+    operations, so the same mask) instead of as a numpy array on the host."""
     grid = np.asarray(grid)
     center = np.asarray(center, dtype=np.float64)
     size = np.asarray(size, dtype=np.float64)
@@ -82,11 +84,26 @@ def crop_mask(grid, center, size, inner_radius, axial_length, crop_ratio=0.95):
     p0 = center - (size - interval) / 2
     p1 = center + (size - interval) / 2
     r = [np.linspace(p0[i], p1[i], grid[i]) for i in range(3)]
+    if device is not None:
+        return _crop_mask_torch(grid, r, inner_radius, axial_length, crop_ratio, device)
     m = np.array(np.meshgrid(r[0], r[1], r[2])).reshape((3, -1)).T
     keep = np.ones(m.shape[0], bool)
     keep[np.sqrt(m[:, 0] ** 2 + m[:, 1] ** 2) > crop_ratio * inner_radius] = False
     keep[np.abs(m[:, 2]) >= axial_length / 2] = False
     return keep.reshape(tuple(grid))
+
+
+def _crop_mask_torch(grid, r, inner_radius, axial_length, crop_ratio, device):
+    nx, ny, nz = (int(g) for g in grid)
+    f = torch.arange(nx * ny * nz, dtype=torch.int64, device=device)
+    # flat index f of the image walks the mesh list in meshgrid 'xy' order (iy, ix, iz)
+    j, i, k = f // (nx * nz), (f // nz) % nx, f % nz
+    x = torch.as_tensor(r[0], dtype=torch.float64, device=device)[i]
+    y = torch.as_tensor(r[1], dtype=torch.float64, device=device)[j]
+    z = torch.as_tensor(r[2], dtype=torch.float64, device=device)[k]
+    keep = torch.sqrt(x * x + y * y) <= crop_ratio * inner_radius
+    keep &= torch.abs(z) < axial_length / 2
+    return keep.reshape(nx, ny, nz)
 
 
 def merge_effmap(total, keep, threshold=1e-6, zero_below=True):
@@ -104,8 +121,7 @@ def merge_effmap(total, keep, threshold=1e-6, zero_below=True):
 def initial_image(grid, center, size, inner_radius, axial_length, device, crop_ratio=0.95):
     """``MasterLoader.create_image`` (src/python/srf/data/loader.py:28-37): ones,
     cropped like the effmap."""
-    keep = torch.as_tensor(crop_mask(grid, center, size, inner_radius, axial_length,
-                                     crop_ratio), device=device)
+    keep = crop_mask(grid, center, size, inner_radius, axial_length, crop_ratio, device=device)
     return keep.to(torch.float32)
 
 

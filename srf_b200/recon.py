@@ -127,8 +127,7 @@ def efficiency_map(model, lors, grid, center, size, inner_radius, axial_length,
             from .data import ListModeDataWithoutTOF
             data = ListModeDataWithoutTOF(part, torch.ones(part.shape[0], device=dev))
         total.add_(map_lors(model, data, img).data)
-    keep = torch.as_tensor(crop_mask(grid, center, size, inner_radius, axial_length,
-                                     crop_ratio), device=dev)
+    keep = crop_mask(grid, center, size, inner_radius, axial_length, crop_ratio, device=dev)
     return Image(merge_effmap(total, keep, threshold, zero_below), center, size), total
 
 
