@@ -989,7 +989,7 @@ def main(argv=None):
                        "-> pinned host image; step k+1's upload overlaps step k"}
 
     # ---------------------------------------------------------------- effmap pass
-    effmap = None
+    effmap = osem = None
     if args.effmap:
         from srf_b200 import recon
         from srf_b200.synthetic import RandomLorSource
@@ -1011,7 +1011,7 @@ def main(argv=None):
                           "map_process -> TOR maplors of each axis group -> crop, normalise, "
                           "invert"}
         if wl.name == "tor_tof_128x128x64_10M" and world == 1:
-            effmap["osem"] = time_osem(model, data, effinv, wl, dev)
+            osem = time_osem(model, data, effinv, wl, dev)
 
     # ---------------------------------------------------------------- roofline
     peaks = {}
@@ -1077,7 +1077,7 @@ def main(argv=None):
                                  % (n_lors * 40 // 10**6),
                            "tuning": args.tuning or "automatic"},
                 "roofline": roof, "cpu_baseline": base, "e2e": e2e,
-                "gpu_launches": gpu_launches, "clocks": clk, "effmap": effmap}
+                "gpu_launches": gpu_launches, "clocks": clk, "effmap": effmap, "osem": osem}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

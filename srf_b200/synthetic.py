@@ -33,23 +33,41 @@ class Sphere:
 
 
 @dataclass
+class Cylinder:
+    """A cylinder parallel to z: axis at (x, y), radius, axial range [z_lo, z_hi]."""
+
+    xy: tuple
+    radius: float
+    z_lo: float
+    z_hi: float
+    activity: float
+
+
+@dataclass
 class Phantom:
-    """A uniform cylinder (axis z) plus spheres; sphere activity replaces the cylinder's."""
+    """A uniform cylinder (axis z) plus inner cylinders, then spheres. Each later shape's
+    activity replaces what lies under it (inner cylinders in list order, then spheres)."""
 
     radius: float = 100.0
     half_length: float = 51.2
     activity: float = 1.0
     spheres: list = field(default_factory=list)
+    cylinders: list = field(default_factory=list)
 
     @property
     def max_activity(self):
-        return max([self.activity] + [s.activity for s in self.spheres])
+        return max([self.activity] + [s.activity for s in self.spheres]
+                   + [c.activity for c in self.cylinders])
 
     def activity_at(self, p):
         """Activity at points p [N,3] (torch)."""
         r2 = p[:, 0] ** 2 + p[:, 1] ** 2
         a = torch.where((r2 <= self.radius ** 2) & (p[:, 2].abs() <= self.half_length),
                         torch.full_like(r2, self.activity), torch.zeros_like(r2))
+        for c in self.cylinders:
+            inside = (((p[:, 0] - c.xy[0]) ** 2 + (p[:, 1] - c.xy[1]) ** 2 <= c.radius ** 2)
+                      & (p[:, 2] >= c.z_lo) & (p[:, 2] <= c.z_hi))
+            a = torch.where(inside, torch.full_like(a, c.activity), a)
         for s in self.spheres:
             c = torch.tensor(s.center, dtype=p.dtype, device=p.device)
             inside = ((p - c) ** 2).sum(1) <= s.radius ** 2
@@ -79,17 +97,22 @@ def standard_phantom(half_length=51.2, radius=100.0):
 
 
 def large_fov_phantom(half_length=500.0, radius=200.0):
-    """Large axial FOV phantom: a cylinder r = 200 mm over the whole axial length with
-    eight spherical inserts along it, four hot (4:1, r = 20 mm) and four cold (activity
-    0, r = 25 mm), alternating around the axis."""
-    spheres = []
+    """Large axial FOV multi-cylinder phantom: a body cylinder r = 200 mm (activity 1)
+    over the whole axial length; an off-centre cylinder r = 60 mm at 2:1 over the
+    central 60 % of it and a cold (activity 0.25) centred cylinder r = 40 mm over the
+    outer axial thirds; and eight cylindrical inserts of 80 mm length along the axis,
+    alternating around it at 120 mm from the centre, four hot (4:1, r = 20 mm) and four
+    cold (activity 0, r = 25 mm)."""
+    cyl = [Cylinder((-70.0, 40.0), 60.0, -0.6 * half_length, 0.6 * half_length, 2.0),
+           Cylinder((0.0, 0.0), 40.0, -half_length, -half_length / 3.0, 0.25),
+           Cylinder((0.0, 0.0), 40.0, half_length / 3.0, half_length, 0.25)]
     for k in range(8):
         z = (k - 3.5) / 4.0 * half_length * 0.9
         ph = k * math.pi / 4.0
         hot = k % 2 == 0
-        spheres.append(Sphere((100.0 * math.cos(ph), 100.0 * math.sin(ph), z),
-                              20.0 if hot else 25.0, 4.0 if hot else 0.0))
-    return Phantom(radius=radius, half_length=half_length, activity=1.0, spheres=spheres)
+        cyl.append(Cylinder((120.0 * math.cos(ph), 120.0 * math.sin(ph)),
+                            20.0 if hot else 25.0, z - 40.0, z + 40.0, 4.0 if hot else 0.0))
+    return Phantom(radius=radius, half_length=half_length, activity=1.0, cylinders=cyl)
 
 
 def random_phantom(seed, half_length, r_lo=60.0, r_hi=150.0):
