@@ -50,9 +50,27 @@ def key_for(grid, patch, n_lors, n_frames=1):
     return f"g{grid[0]}x{grid[1]}x{grid[2]}_p{patch}_n2^{bucket}_f{n_frames}"
 
 
+def cuda_event_time(step, warmup, reps):
+    """Mean milliseconds of ``step()`` over ``reps`` runs after ``warmup`` untimed runs,
+    with CUDA events on the current stream."""
+    for _ in range(warmup):
+        step()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    for _ in range(reps):
+        step()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
 class Autotuner:
-    def __init__(self, cache_path=None):
+    """``timer(step, warmup, reps) -> ms`` measures one candidate (default: CUDA events)."""
+
+    def __init__(self, cache_path=None, timer=None):
         self.cache_path = cache_path
+        self.timer = timer or cuda_event_time
         self.table = {}
         if cache_path and os.path.exists(cache_path):
             with open(cache_path) as f:
@@ -66,16 +84,7 @@ class Autotuner:
         timings = {}
         for c in cands:
             set_tuning(*c)
-            for _ in range(warmup):
-                step()
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            s.record()
-            for _ in range(reps):
-                step()
-            e.record()
-            torch.cuda.synchronize()
-            timings[c] = s.elapsed_time(e) / reps
+            timings[c] = self.timer(step, warmup, reps)
         best = min(timings, key=timings.get)
         self.table[key] = best
         set_tuning(*best)
