@@ -83,8 +83,9 @@ def parse_args(argv=None):
                          "batched OSEM iteration vs the plain per-frame loop")
     ap.add_argument("--frames", type=int, default=64)
     ap.add_argument("--no-order", dest="order", action="store_false",
-                    help="keep the preprocessed records in recon_process order instead of "
-                         "grouping similar directions (preprocess.order_by_direction)")
+                    help="keep the preprocessed records in recon_process order, and the "
+                         "effmap's map records in map_process order, instead of grouping "
+                         "similar directions (preprocess.order_by_direction)")
     ap.add_argument("--separate-ops", dest="combined", action="store_false",
                     help="run projection and back-projection as two library calls (the "
                          "reference's op sequence) instead of the combined TOR call")
@@ -192,9 +193,10 @@ def run_large_recon(args):
     args_e = (list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
               wl.scanner.axial_length)
     recon.efficiency_map(model, S.RandomLorSource(chunk, wl.scanner, 78, device=dev),
-                         *args_e)  # warm-up: one chunk (sizes the scratch pool)
+                         *args_e, order=args.order)  # warm-up: one chunk (sizes the scratch pool)
     (effinv, _), effmap_ms = timed(lambda: recon.efficiency_map(
-        model, S.RandomLorSource(wl.n_effmap, wl.scanner, 77, device=dev), *args_e))
+        model, S.RandomLorSource(wl.n_effmap, wl.scanner, 77, device=dev), *args_e,
+        order=args.order))
     x0 = _image_of(initial_image(list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
                                  wl.scanner.axial_length, dev), wl)
     osem, setup_ms = timed(lambda: recon.OSEM(model, data, effinv, x0, n_subsets=wl.subsets))
@@ -996,20 +998,21 @@ def main(argv=None):
         args_e = (list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
                   wl.scanner.axial_length)
         recon.efficiency_map(model, RandomLorSource(16_000_000, wl.scanner, 78, device=dev),
-                             *args_e)  # warm-up: one full chunk (sizes the scratch pool)
+                             *args_e, order=args.order)  # warm-up: one full chunk
         src = RandomLorSource(wl.n_effmap, wl.scanner, 77, device=dev)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        effinv, _ = recon.efficiency_map(model, src, *args_e)
+        effinv, _ = recon.efficiency_map(model, src, *args_e, order=args.order)
         e1.record()
         torch.cuda.synchronize()
         e_ms = max_over_ranks(e0.elapsed_time(e1), world)
         effmap = {"lors": wl.n_effmap, "ms": e_ms, "lors_per_s": wl.n_effmap / (e_ms / 1e3),
                   "chunk": src.chunk,
                   "path": "random crystal pairs generated on the device per chunk -> "
-                          "map_process -> TOR maplors of each axis group -> crop, normalise, "
-                          "invert"}
+                          "map_process -> " + ("records ordered by direction -> "
+                                               if args.order else "")
+                          + "TOR maplors of each axis group -> crop, normalise, invert"}
         if wl.name == "tor_tof_128x128x64_10M" and world == 1:
             osem = time_osem(model, data, effinv, wl, dev)
 

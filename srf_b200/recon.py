@@ -100,13 +100,17 @@ def order_subset(model, data, image):
 
 
 def efficiency_map(model, lors, grid, center, size, inner_radius, axial_length,
-                   chunk=16_000_000, crop_ratio=0.95, threshold=1e-6, zero_below=True):
+                   chunk=16_000_000, crop_ratio=0.95, threshold=1e-6, zero_below=True,
+                   order=True):
     """Inverted efficiency map from detector-pair LORs: Maplors summed over the axis
     groups (or Siddon map), cropped, normalised to max 1 and inverted
     (merge_map.py:37-41). ``lors`` is an [N, 6] CUDA tensor, or a source with ``len()``
     and ``source(start, count)`` returning [count, 6] CUDA chunks (for example
     ``synthetic.RandomLorSource``), so that N LORs never exist at once; its chunk size
-    then sets ``chunk``."""
+    then sets ``chunk``. With ``order`` (TOR model) each chunk's map records are
+    reordered by direction inside 4096-record blocks (``preprocess.order_by_direction``)
+    before Maplors: the map is the same sum taken in another order, and the slab kernels
+    walk fewer voxel slots for LORs of mixed directions (random detector pairs)."""
     if callable(lors):
         n = len(lors)
         chunk = getattr(lors, "chunk", chunk)
@@ -122,6 +126,9 @@ def efficiency_map(model, lors, grid, center, size, inner_radius, axial_length,
         part = take(s, min(chunk, n - s))
         if isinstance(model, SplitLoRsModel):
             groups = map_process(part)
+            if order:
+                from .preprocess import order_by_direction
+                groups = order_by_direction(groups)
             data = split_listmode(groups, without_tof=True)
         else:
             from .data import ListModeDataWithoutTOF

@@ -445,3 +445,22 @@ def test_tor_osem_subsets_ordered_equals_unordered():
         o.step()
         out.append(o.x.data)
     assert float((out[1] - out[0]).norm() / out[0].norm()) < 1e-6
+
+
+def test_effmap_record_order_changes_only_summation_order():
+    """Map records reordered by direction inside each chunk (the default) give the map of
+    the records in map_process order, up to float summation order."""
+    from srf_b200 import SplitLoRsModel
+    from srf_b200 import recon
+    from srf_b200.synthetic import random_lors
+    from tests import _cases as K
+    grid, voxel = (64, 64, 32), 6.4
+    size = [g * voxel for g in grid]
+    model = SplitLoRsModel(K.KW_CONFIG, False)
+    lors = random_lors(300_000, K.SCANNER, 11, device="cuda")
+    args = (list(grid), [0, 0, 0], size, K.SCANNER.inner_radius, K.SCANNER.axial_length)
+    ea, a = recon.efficiency_map(model, lors, *args, chunk=120_000, order=True)
+    eb, b = recon.efficiency_map(model, lors, *args, chunk=120_000, order=False)
+    assert torch.count_nonzero(b) > 0
+    assert float((a - b).norm() / b.norm()) < 1e-6
+    assert float((ea.data - eb.data).norm() / eb.data.norm()) < 1e-5
