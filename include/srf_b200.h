@@ -174,7 +174,9 @@ int srf_tor_backproject_adjoint_batched(const float *x1, const float *y1, const 
  * autotuner; affects later calls from every thread). path: 0 automatic, 1 shared-memory
  * slab kernels with one lane per (LOR, slab) segment, 2 LOR-centric kernels (L2 gathers,
  * global atomics), 3 slab kernels with a segment's slices spread over lanes; slab_slices: slices
- * per slab, 0 = as many as fit; grid_mult: persistent slab CTAs = SMs x grid_mult (1..8). */
+ * per slab, 0 = as many as fit; grid_mult: persistent slab CTAs = SMs x grid_mult (1..8;
+ * 0 = automatic: 2 for projection and back-projection launches of at least 4M LORs over
+ * whole-slice slabs, else 1). */
 int srf_tor_set_tuning(int path, int slab_slices, int grid_mult);
 
 /* No counterpart in the reference: upper bound, in bytes, of the per-slab LOR lists the

@@ -4,7 +4,8 @@
 (``srf_tor_set_tuning``): the kernel family (0 automatic, 1 shared-memory slabs with a
 lane per (LOR, slab) segment, 2 LOR-centric, 3 shared-memory slabs with a segment's
 slices spread over lanes), the number of slices per shared-memory slab (0 = as many as fit) and
-the grid multiplier of the persistent slab kernel.
+the grid multiplier of the persistent slab kernel (0 = automatic). ``set_tuning()``
+restores the library's defaults (all automatic).
 
 ``Autotuner`` times a caller-supplied step (for example one OSEM sub-iteration on a
 representative subset) under each candidate setting with CUDA events and keeps the
@@ -20,10 +21,10 @@ import torch
 
 from . import _lib
 
-DEFAULT = (0, 0, 1)
+DEFAULT = (0, 0, 0)
 
 
-def set_tuning(path=0, slab_slices=0, grid_mult=1):
+def set_tuning(path=0, slab_slices=0, grid_mult=0):
     _lib.call("srf_tor_set_tuning", int(path), int(slab_slices), int(grid_mult))
     return (path, slab_slices, grid_mult)
 

@@ -75,7 +75,8 @@ def tcase():
 # every slice into bands of rows, slabs with a segment's slices spread over lanes (3), and
 # LOR-centric kernels reading the image from L2 with global atomics (2, the fallback when
 # nothing fits in shared memory).
-TOR_PATHS = {"slab": (1, 0), "slab_bands": (1, 16), "slab_spread": (3, 0), "global": (2, 0)}
+TOR_PATHS = {"slab": (1, 0), "slab_grid2": (1, 0, 2), "slab_bands": (1, 16),
+             "slab_spread": (3, 0), "global": (2, 0)}
 
 
 @pytest.fixture(params=list(TOR_PATHS))

@@ -72,7 +72,8 @@ def test_tune_picks_fastest_and_caches(tmp_path, recorder):
 
 
 def test_invalid_settings_rejected():
-    for bad in [(4, 0, 1), (-1, 0, 1), (1, -1, 1), (1, 0, 0), (1, 0, 9)]:
+    for bad in [(4, 0, 1), (-1, 0, 1), (1, -1, 1), (1, 0, -1), (1, 0, 9)]:
         with pytest.raises(_lib.SRFError):
             tuning.set_tuning(*bad)
+    tuning.set_tuning(1, 0, 0)  # grid multiplier 0: automatic
     tuning.set_tuning()
