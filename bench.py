@@ -91,6 +91,9 @@ def parse_args(argv=None):
                          "reference's op sequence) instead of the combined TOR call")
     ap.add_argument("--no-effmap", dest="effmap", action="store_false",
                     help="skip timing the efficiency-map pass (random detector pairs)")
+    ap.add_argument("--no-variants", dest="variants", action="store_false",
+                    help="skip the config variants of the same step (the reference preset "
+                         "kernel_width 4.0; the geometric sigma2 factor on)")
     ap.add_argument("--tuning", default=None,
                     help="PATH,SLAB_SLICES,GRID_MULT for srf_tor_set_tuning (default: the "
                          "library's automatic choice)")
@@ -104,6 +107,31 @@ def project_back(model, image, data, combined=True):
     if combined:
         return projection_backprojection(model, image, data)[1]
     return backprojection(model, projection(model, image, data), image)
+
+
+def time_variants(wl, data, image, tof_bin, tof_sigma2, combined, world, steps=5, warmup=3):
+    """The timed step under the workload's variants: the reference preset's
+    kernel_width 4.0 (resource/recon_task.json:46; window 3 x 3 at 3.2 mm) and the
+    geometric sigma2 factor switched on (geo_sigma2_flag, the TOR sigma scaled per LOR).
+    Same events, image and TOF; CUDA events, max over ranks."""
+    from srf_b200 import SplitLoRsModel
+    out = {}
+    n = sum(data[a].lors.shape[0] for a in "xyz")
+    for name, kw, geo in (("kw4", 4.0, False), ("geo", wl.kernel_width, True)):
+        m = SplitLoRsModel(kw, geo, tof_sigma2=tof_sigma2, tof_bin=tof_bin)
+        for _ in range(warmup):
+            project_back(m, image, data, combined)
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(steps):
+            project_back(m, image, data, combined)
+        s1.record()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(s0.elapsed_time(s1), world) / steps
+        out[name] = {"kernel_width": kw, "geo_sigma2_flag": geo, "steps": steps,
+                     "ms_per_step": ms, "value": n * world / (ms / 1e3), "unit": UNIT}
+    return out
 
 
 def time_osem(model, data, effinv, wl, dev, warmup=1):
@@ -392,35 +420,132 @@ def algorithmic_work(model, data, image):
     return per
 
 
-def roofline_components(kernel, ms_per_step, alg_bytes, n_lors, rec, useful, slots, hbm_peak,
-                        probe):
-    """Bound time of the dominant op per step as the slowest of three measured limits:
-    HBM (algorithmic bytes / measured copy bandwidth), L2 (the same bytes / the measured
-    L2 read bandwidth) and SFU (one exp per non-zero-weight sample / measured ex2 rate);
-    frac = bound / measured. The reference's own exp count (one TOF exp per window
-    sample plus one geometric exp per non-zero sample) is given for comparison."""
-    t_hbm = alg_bytes / (hbm_peak * 1e9)
-    t_l2 = alg_bytes / (probe["l2_gbs"] * 1e9)
-    t_sfu = useful / probe["ex2_per_s"]
+OPS_OF = {"srf_tor_projection": ("proj",), "srf_tor_backprojection": ("back",),
+          "srf_tor_projection_backprojection": ("proj", "back")}
+
+
+def roofline_components(kernel, ms_per_step, n_lors, n_groups, rec, useful, slots, image_bytes,
+                        hbm_peak, probe):
+    """Bound time T* of the dominant op per step, as the survey's measurement section
+    defines it, T* = max(B_HBM / HBM peak, B / L2 peak, exps / SFU peak):
+
+    * B_HBM: the bytes that must cross HBM: each LOR record (``rec`` bytes) and its value
+      (4 B: the projection's output, the back-projection's input) once per op, the image
+      of each axis group once per op (read by the projection, read-modify-written by the
+      back-projection);
+    * B: B_HBM plus the voxel samples: 4 B per useful (non-zero-weight) sample read by
+      the projection, 8 B per useful sample read-modify-written by the back-projection;
+    * exps: one per useful sample and op;
+
+    each against its measured peak (HBM copy; L2 read, ex2 and shared-memory probes run
+    in the same process); frac = T* / T. The slab kernels serve their samples from shared
+    memory, so two shared-memory terms are reported beside the survey's three: sample
+    bytes / measured shared read bandwidth, and back-projected samples / measured
+    shared-memory atomicAdd rate at hashed addresses."""
+    ops_ = OPS_OF.get(kernel, ("proj",))
+    b_hbm = b_samp = 0
+    n_atom = 0
+    for op in ops_:
+        b_hbm += n_lors * (rec + 4) + n_groups * image_bytes * (1 if op == "proj" else 2)
+        b_samp += useful * (4 if op == "proj" else 8)
+        n_atom += useful if op == "back" else 0
+    exps = useful * len(ops_)
     t_meas = ms_per_step / 1e3
-    bound = max(t_hbm, t_l2, t_sfu)
-    # bytes per window sample: image read (projection), read-modify-write (back-projection)
-    per = {"srf_tor_backprojection": 8, "srf_tor_projection_backprojection": 12}.get(kernel, 4)
-    lor_passes = 2 if kernel == "srf_tor_projection_backprojection" else 1
-    return {
-        "hbm": {"ms": t_hbm * 1e3, "frac": t_hbm / t_meas, "peak_gbs": hbm_peak},
-        "l2": {"ms": t_l2 * 1e3, "frac": t_l2 / t_meas, "peak_gbs": probe["l2_gbs"]},
-        "sfu": {"ms": t_sfu * 1e3, "frac": t_sfu / t_meas, "peak_ex2_per_s": probe["ex2_per_s"],
-                "exps": useful, "reference_exps": useful + slots},
-        "bound_ms": bound * 1e3, "measured_ms": ms_per_step, "frac_of_bound": bound / t_meas,
-        "window_sample_bytes": lor_passes * n_lors * (rec + 4) + per * slots,
-        "window_sample_frac_hbm": (lor_passes * n_lors * (rec + 4) + per * slots)
-                                  / (hbm_peak * 1e9) / t_meas,
-        "probe": probe["method"],
+    terms = {
+        "hbm": (b_hbm / (hbm_peak * 1e9), {"bytes": b_hbm, "peak_gbs": hbm_peak}),
+        "l2": ((b_hbm + b_samp) / (probe["l2_gbs"] * 1e9),
+               {"bytes": b_hbm + b_samp, "peak_gbs": probe["l2_gbs"]}),
+        "sfu": (exps / probe["ex2_per_s"], {"exps": exps, "peak_ex2_per_s": probe["ex2_per_s"],
+                                            "reference_exps": (useful + slots) * len(ops_)}),
     }
+    side = {
+        "smem_read": (b_samp / (probe["smem_gbs"] * 1e9),
+                      {"bytes": b_samp, "peak_gbs": probe["smem_gbs"]}),
+        "smem_atomic": (n_atom / probe["smem_atomic_random_per_s"],
+                        {"atomics": n_atom,
+                         "peak_per_s": probe["smem_atomic_random_per_s"],
+                         "peak_per_s_conflict_free": probe["smem_atomic_per_s"]}),
+    }
+    out = {}
+    for k, (t, extra) in list(terms.items()) + list(side.items()):
+        out[k] = dict(ms=t * 1e3, frac=t / t_meas, **extra)
+    bound_term = max(terms, key=lambda k: terms[k][0])
+    bound = terms[bound_term][0]
+    out.update({"bound_term": bound_term, "bound_ms": bound * 1e3, "measured_ms": ms_per_step,
+                "frac_of_bound": bound / t_meas, "b_hbm": b_hbm, "b_total": b_hbm + b_samp,
+                "probe": probe["method"]})
+    return out
+
+
+def roofline(kern, steps, n_lors, n_groups, useful, slots, image_bytes, hbm_peak, peak_src,
+             workload):
+    """The line's ``roofline`` object for the dominant op (most device time in the timed
+    region): its bound T* (``roofline_components``) expressed in the binding term's units
+    (``achieved`` = that term's bytes, or exps, per launch / the launch's mean CUDA-event
+    time; ``frac`` = achieved / peak = T* / T), the other terms, and ``traffic``, the
+    DRAM bytes per launch ncu measured for this workload (profiles/roofline_traffic.txt)."""
+    from srf_b200 import profiling
+    if not kern:
+        return None
+    dom = max(kern, key=lambda k: kern[k]["total_ms"])
+    launches = kern[dom]["launches"]
+    comp = roofline_components(dom, kern[dom]["total_ms"] / steps, n_lors, n_groups, 40,
+                               useful, slots, image_bytes, hbm_peak, profiling.measure_peaks())
+    term = comp["bound_term"]
+    per_launch = steps / max(launches, 1)
+    mean_s = kern[dom]["mean_ms"] / 1e3
+    if term == "sfu":
+        achieved = comp["sfu"]["exps"] * per_launch / mean_s / 1e12
+        peak, unit = comp["sfu"]["peak_ex2_per_s"] / 1e12, "Texp/s"
+    else:
+        achieved = comp[term]["bytes"] * per_launch / mean_s / 1e9
+        peak, unit = comp[term]["peak_gbs"], "GB/s"
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    if os.path.exists(prof):  # measured per workload; null where not captured
+        traffic = json.load(open(prof)).get(workload, {}).get(dom)
+    return {"kernel": dom, "bound": term, "achieved": achieved, "peak": peak, "unit": unit,
+            "frac": achieved / peak, "traffic": traffic,
+            "peak_source": f"{peak_src} hbm_gbs (burst copy) for the HBM term; L2, ex2 and "
+                           "shared-memory peaks from the library's probes in this run",
+            "b_hbm_per_launch": comp["b_hbm"] * per_launch,
+            "algorithmic_bytes_per_launch": comp["b_total"] * per_launch,
+            "useful_samples_per_step": useful, "window_samples_per_step": slots,
+            "components": comp,
+            "kernel_ms": {k: {"launches": v["launches"], "mean_ms": v["mean_ms"],
+                              "share": v["total_ms"] / sum(x["total_ms"] for x in kern.values())}
+                          for k, v in kern.items()}}
 
 
 # ------------------------------------------------------------------ CPU baseline
+
+
+def host_cpu():
+    """The host the CPU baseline runs on: lscpu's model name, core and thread counts and
+    clock (current and maximum MHz), /proc/cpuinfo when lscpu is absent."""
+    info = {"nproc": os.cpu_count()}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        want = {"Model name": "model", "CPU(s)": "cpus", "Thread(s) per core": "threads_per_core",
+                "Core(s) per socket": "cores_per_socket", "Socket(s)": "sockets",
+                "CPU MHz": "mhz", "CPU max MHz": "max_mhz"}
+        for ln in out.splitlines():
+            k, _, v = ln.partition(":")
+            if k.strip() in want:
+                info[want[k.strip()]] = v.strip()
+    except (OSError, subprocess.SubprocessError):
+        pass
+    if "model" not in info or "mhz" not in info:
+        try:
+            for ln in open("/proc/cpuinfo"):
+                k, _, v = ln.partition(":")
+                if k.strip() == "model name":
+                    info.setdefault("model", v.strip())
+                elif k.strip() == "cpu MHz":
+                    info.setdefault("mhz", v.strip())
+        except OSError:
+            pass
+    return info
 
 
 def cpu_baseline(groups_host, wl, tof_bin, tof_sigma2, image_np, target_s):
@@ -464,7 +589,7 @@ def cpu_baseline(groups_host, wl, tof_bin, tof_sigma2, image_np, target_s):
     n0, t0 = run(2000.0 / total)  # calibration
     frac = min(1.0, (2000.0 / total) * max(1.0, target_s / max(t0, 1e-3)))
     n1, t1 = run(frac)
-    return {"value": n1 / t1, "unit": UNIT, "cores": threads, "kind": kind,
+    return {"value": n1 / t1, "unit": UNIT, "cores": threads, "kind": kind, "host": host_cpu(),
             "sample": f"{n1} LORs (first {frac * 100:.2f}% of each dominant-axis group of the "
                       f"same preprocessed events), projection + back-projection, "
                       f"{t1:.1f} s wall"}
@@ -652,6 +777,7 @@ def siddon_cpu_baseline(events, model, image, target_s):
     k = int(min(len(ev), k * max(1.0, target_s / max(t, 1e-3))))
     t = run(k)
     return {"value": k / t, "unit": UNIT, "cores": threads, "kind": "reference",
+            "host": host_cpu(),
             "sample": f"first {k} events ({int((visits[:k] > 0).sum())} visit the image), "
                       f"projection + back-projection, {t:.1f} s wall"}
 
@@ -788,7 +914,7 @@ def run_reference(args):
                        "kernel_width": wl.kernel_width, "tof_res_ps": wl.tof_res_ps,
                        "sample_lors_per_step": n // args.steps},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
-                             "kind": "reference" if use_ref else "port",
+                             "kind": "reference" if use_ref else "port", "host": host_cpu(),
                              "sample": f"{n // args.steps} LORs per step from the same "
                                        f"preprocessed events"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -990,6 +1116,10 @@ def main(argv=None):
                "path": "pinned host events -> recon_process -> projection -> backprojection "
                        "-> pinned host image; step k+1's upload overlaps step k"}
 
+    variants = None
+    if args.variants:
+        variants = time_variants(wl, data, image, tof_bin, tof_sigma2, args.combined, world)
+
     # ---------------------------------------------------------------- effmap pass
     effmap = osem = None
     if args.effmap:
@@ -1025,36 +1155,10 @@ def main(argv=None):
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     useful = sum(w["useful"] for w in work.values())
     slots = sum(w["slots"] for w in work.values())
-    rec = 40  # bytes of one preprocessed LOR record (10 float32)
-    alg = {"srf_tor_projection": n_lors * (rec + 4) + 4 * useful,
-           "srf_tor_backprojection": n_lors * (rec + 4) + 8 * useful}
-    # the combined call runs both ops: each reads the records once, the values pass
-    # through HBM once each way, and every useful sample is read then read-modify-written
-    alg["srf_tor_projection_backprojection"] = (alg["srf_tor_projection"]
-                                                + alg["srf_tor_backprojection"])
-    roof = None
-    peaks_probe = profiling.measure_peaks() if kern else None
-    if kern:
-        dom = max(kern, key=lambda k: kern[k]["total_ms"])
-        launches = kern[dom]["launches"]
-        per_launch_bytes = alg.get(dom, 0) * args.steps / max(launches, 1)
-        achieved = per_launch_bytes / (kern[dom]["mean_ms"] / 1e3) / 1e9
-        traffic = None
-        prof = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
-        if os.path.exists(prof):  # measured per workload; null where not captured
-            traffic = json.load(open(prof)).get(wl.name, {}).get(dom)
-        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
-                "peak_source": f"{peak_src} hbm_gbs (burst copy)",
-                "algorithmic_bytes_per_launch": per_launch_bytes,
-                "useful_samples_per_step": useful,
-                "window_samples_per_step": slots,
-                "components": roofline_components(dom, kern[dom]["total_ms"] / args.steps,
-                                                  alg[dom], n_lors, rec, useful, slots,
-                                                  hbm_peak, peaks_probe),
-                "kernel_ms": {k: {"launches": v["launches"], "mean_ms": v["mean_ms"],
-                                  "share": v["total_ms"] / sum(x["total_ms"] for x in kern.values())}
-                              for k, v in kern.items()}}
+    n_groups = sum(1 for w in work.values() if w["lors"] > 0)
+    image_bytes = int(np.prod(wl.grid)) * 4
+    roof = roofline(kern, args.steps, n_lors, n_groups, useful, slots, image_bytes, hbm_peak,
+                    peak_src, wl.name)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1080,7 +1184,8 @@ def main(argv=None):
                                  % (n_lors * 40 // 10**6),
                            "tuning": args.tuning or "automatic"},
                 "roofline": roof, "cpu_baseline": base, "e2e": e2e,
-                "gpu_launches": gpu_launches, "clocks": clk, "effmap": effmap, "osem": osem}
+                "gpu_launches": gpu_launches, "clocks": clk, "variants": variants,
+                "effmap": effmap, "osem": osem}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -136,8 +136,10 @@ int srf_tor_projection_backprojection_batched(
 
 /* No counterpart in the reference: batched TOR for many reconstructions that share one
  * geometry (dynamic frames, many phantoms). LOR i belongs to frame frame[i] (DEVICE
- * int32[N], 0 <= frame[i] < n_frames); images are n_frames consecutive blocks of
- * frame_stride floats (>= grid voxels). One launch covers every frame. Semantics per
+ * int32[N], 0 <= frame[i] < n_frames; a LOR with a frame id outside that range
+ * contributes nothing, as a LOR with non-finite endpoints does); images are n_frames
+ * consecutive blocks of frame_stride floats (>= grid voxels). One launch covers every
+ * frame. Semantics per
  * frame are those of srf_tor_projection / srf_tor_backprojection /
  * srf_tor_backproject_adjoint; `accumulate` = 0 zeroes all n_frames blocks first. */
 int srf_tor_projection_batched(const float *x1, const float *y1, const float *z1,
@@ -267,7 +269,10 @@ int srf_recon_process(const float *events, int64_t num_events, int64_t event_str
  *     capture;
  *   - all calls on a device share the buffer and it keeps the last call's contents
  *     (no part needs to start at zero); calls that overlap on the GPU race on it, so
- *     serialise them on one stream.
+ *     serialise them on one stream;
+ *   - the looked-up address is kept for the life of the process, like the library's
+ *     other per-device state (its scratch pool): after cudaDeviceReset of a device,
+ *     do not call the library on that device again in the same process.
  * Same inputs, outputs and results as srf_recon_process. */
 #define SRF_RECON_PROCESS_NOALLOC_MAX_EVENTS 8388608
 int srf_recon_process_noalloc(const float *events, int64_t num_events, int64_t event_stride,
@@ -316,6 +321,14 @@ int srf_csr_spmm(const int64_t *rowptr, const int *col, const float *val, int64_
 int srf_probe_threads(int64_t *n_threads);
 int srf_probe_l2_read(const float *buf, int64_t n_floats, int reps, float *sink, void *stream);
 int srf_probe_ex2(int iters, float *sink, void *stream);
+/* srf_probe_smem_threads: threads per shared-memory probe launch (the length of `sink`).
+ * srf_probe_smem_read: every thread reads 16 bytes from a 32 KB shared buffer `iters`
+ * times (a warp on consecutive addresses).
+ * srf_probe_smem_atomic: every thread does `iters` float atomicAdd into a 32 KB shared
+ * buffer; random = 0: a warp's lanes on 32 consecutive floats, 1: hashed addresses. */
+int srf_probe_smem_threads(int64_t *n_threads);
+int srf_probe_smem_read(int iters, float *sink, void *stream);
+int srf_probe_smem_atomic(int iters, int random, float *sink, void *stream);
 
 #ifdef __cplusplus
 }

@@ -20,7 +20,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
-DEFAULT_REFERENCE = "/root/reference"
+# the SRF checkout: $SRF_REFERENCE, else its location in the build container
+DEFAULT_REFERENCE = os.environ.get("SRF_REFERENCE", "/root/reference")
 
 _f = C.c_float
 _i64 = C.c_int64

@@ -64,6 +64,9 @@ SIGNATURES = {
     "srf_probe_threads": ([_p], _int),
     "srf_probe_l2_read": ([_p, _i64, _int, _p, _p], _int),
     "srf_probe_ex2": ([_int, _p, _p], _int),
+    "srf_probe_smem_threads": ([_p], _int),
+    "srf_probe_smem_read": ([_int, _p, _p], _int),
+    "srf_probe_smem_atomic": ([_int, _int, _p, _p], _int),
 }
 
 

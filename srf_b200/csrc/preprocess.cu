@@ -368,7 +368,8 @@ extern "C" int srf_map_process(const float *lors, int64_t num_lors, int64_t lor_
 // * Host code cannot use the array's name as a device address, so the first call on
 //   each device (with that device current) asks the runtime for the address with
 //   cudaGetSymbolAddress and caches it; that first call should therefore happen before
-//   any stream capture.
+//   any stream capture. The cache lives as long as the process: after cudaDeviceReset
+//   the address is stale, and the library must not be called on that device again.
 // * All calls on a device share the one buffer and it keeps the last call's contents.
 //   Nothing in it needs to start at zero: every byte a call reads was written earlier
 //   in the same call. Calls whose kernels overlap on the GPU (concurrent streams, or
@@ -405,7 +406,8 @@ int noalloc_scratch(void **ptr) {
     if (!g_noalloc_ptr[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
+        if (e == cudaSuccess && !p) e = cudaErrorInvalidSymbol;  // never a null address
+        if (e != cudaSuccess) {
             set_cuda_error(e);
             return SRF_ERR_CUDA;
         }

@@ -75,6 +75,12 @@ __device__ __forceinline__ int64_t frame_offset(const TorParams &p, int64_t t) {
     return p.frame ? (int64_t)__ldg(p.frame + t) * p.frame_stride : 0;
 }
 
+// Batched calls: a LOR whose frame id lies outside [0, n_frames) contributes nothing
+// (as a LOR with non-finite endpoints does) instead of indexing past the image stack.
+__device__ __forceinline__ bool frame_ok(const TorParams &p, int64_t t) {
+    return !p.frame || (unsigned)__ldg(p.frame + t) < (unsigned)p.n_frames;
+}
+
 // slice_z of the reference launchers: float for projection (tor.cu.cc:380), a double
 // intermediate for back-projection and map (:423, :471).
 template <int OP>
@@ -97,6 +103,11 @@ __device__ __forceinline__ float fast_exp2(float x) {
 // for map calls whose divisor is zero or non-finite.
 template <int OP>
 __device__ __noinline__ void generic_lor(const TorParams &p, int64_t t, int lane) {
+    if (!frame_ok(p, t)) {
+        if (OP == kProj && lane == 0) p.proj_out[t] = 0.0f;
+        if (OP == kCount && lane == 0) p.count_out[t] = p.count_out[p.n + t] = 0;
+        return;
+    }
     const int64_t slice_mesh = (int64_t)p.gx * p.gy;
     const int64_t img0 = frame_offset(p, t);
     const int64_t o = t * p.stride;
@@ -252,6 +263,7 @@ struct LorConst {
 template <int OP>
 __device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorConst &L) {
     L.all = false;
+    if (!frame_ok(p, t)) return false;
     const int64_t o = t * p.stride;
     const float x1 = __ldg(p.x1 + o), y1 = __ldg(p.y1 + o), z1 = __ldg(p.z1 + o);
     const float x2 = __ldg(p.x2 + o), y2 = __ldg(p.y2 + o), z2 = __ldg(p.z2 + o);
@@ -654,7 +666,7 @@ __global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams 
         const int64_t t = base + (int64_t)it * kSegThreads + threadIdx.x;
         if (t >= p.n) break;
         int s_lo, s_hi, packed = -1;
-        bool ok = lor_slices(p, t, s_lo, s_hi);
+        bool ok = frame_ok(p, t) && lor_slices(p, t, s_lo, s_hi);
         if (ok && OP == kBack) ok = (double)__ldg(p.values + t) > 1e-7;  // tor.cu.cc:203
         if (ok) {
             const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;

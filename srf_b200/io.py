@@ -85,8 +85,11 @@ def stream_events(source, chunk=16_000_000, device=None):
     """Yield the rows of ``source`` (a path or an [N, C] array) as contiguous float32 CUDA
     tensors of at most ``chunk`` rows, in order. Two pinned host buffers alternate: chunk
     k+1 is copied into one and uploaded on a separate stream while the caller works on
-    chunk k (each yielded tensor is ready on the current stream). A yielded tensor stays
-    valid until the generator is advanced twice."""
+    chunk k (each yielded tensor is ready on the current stream). Three device buffers
+    rotate, so a yielded tensor stays valid until the generator is advanced twice: the
+    caller may hold chunk k while it works on chunk k+1 (neighbouring chunks in pairs).
+    Clone a chunk to keep it longer (``list(stream_events(...))`` without cloning
+    would hold aliases of the three buffers)."""
     arr = load_listmode(source) if isinstance(source, (str, os.PathLike)) else source
     if arr.ndim != 2:
         raise ValueError("source must be an [N, C] array")
@@ -96,31 +99,35 @@ def stream_events(source, chunk=16_000_000, device=None):
         return
     rows = min(chunk, n)
     pinned = [torch.empty((rows, c), dtype=torch.float32).pin_memory() for _ in range(2)]
-    gpu = [torch.empty((rows, c), dtype=torch.float32, device=dev) for _ in range(2)]
+    n_dev = min(3, (n + rows - 1) // rows)
+    gpu = [torch.empty((rows, c), dtype=torch.float32, device=dev) for _ in range(n_dev)]
     copy = torch.cuda.Stream(device=dev)
-    done = [None, None]
+    staged = [None, None]  # per pinned buffer: its last upload's event
+    ready = [None] * n_dev  # per device buffer: the event of the upload it holds
     bounds = chunk_bounds(n, rows)
 
     def upload(k):
         s, e = bounds[k]
-        b = k % 2
-        if done[b] is not None:
-            done[b].synchronize()  # the pinned buffer's previous upload has finished
-        pinned[b][: e - s].numpy()[:] = arr[s:e]
+        h, d = k % 2, k % n_dev
+        if staged[h] is not None:
+            staged[h].synchronize()  # the pinned buffer's previous upload has finished
+        pinned[h][: e - s].numpy()[:] = arr[s:e]
         with torch.cuda.stream(copy):
-            copy.wait_stream(torch.cuda.current_stream(dev))  # caller done with gpu[b]
-            gpu[b][: e - s].copy_(pinned[b][: e - s], non_blocking=True)
+            # the caller's work queued so far (on chunks up to k-1) is done with gpu[d],
+            # which last held chunk k-3
+            copy.wait_stream(torch.cuda.current_stream(dev))
+            gpu[d][: e - s].copy_(pinned[h][: e - s], non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(copy)
-        done[b] = ev
+        staged[h] = ready[d] = ev
 
     upload(0)
     for k in range(len(bounds)):
         if k + 1 < len(bounds):
             upload(k + 1)
         s, e = bounds[k]
-        torch.cuda.current_stream(dev).wait_event(done[k % 2])
-        yield gpu[k % 2][: e - s]
+        torch.cuda.current_stream(dev).wait_event(ready[k % n_dev])
+        yield gpu[k % n_dev][: e - s]
 
 
 def load_split(lors_path, tof_res, emap_path=None, center=None, size=None, chunk=16_000_000,

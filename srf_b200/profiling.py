@@ -65,11 +65,14 @@ def timed_call(name, stream):
         t.records.append((name, s, e))
 
 
-def measure_peaks(device=None, l2_mib=48, l2_reps=20, ex2_iters=4096):
-    """Measured L2 read bandwidth (GB/s) and ex2 throughput (per second) of this GPU,
-    from the library's probe kernels (``srf_probe_l2_read``, ``srf_probe_ex2``): one
-    warm-up and one timed launch each, CUDA events on the current stream. The L2 buffer
-    (default 48 MiB) stays resident in the 126 MB L2."""
+def measure_peaks(device=None, l2_mib=48, l2_reps=20, ex2_iters=4096, smem_iters=8192,
+                  atomic_iters=2048):
+    """Measured L2 read bandwidth (GB/s), ex2 throughput (per second), shared-memory read
+    bandwidth (GB/s) and shared-memory float atomicAdd rates (per second; lanes on
+    distinct banks, and hashed addresses) of this GPU, from the library's probe kernels
+    (``srf_probe_l2_read``, ``srf_probe_ex2``, ``srf_probe_smem_read``,
+    ``srf_probe_smem_atomic``): one warm-up and one timed launch each, CUDA events on the
+    current stream. The L2 buffer (default 48 MiB) stays resident in the 126 MB L2."""
     import ctypes
 
     from . import _lib
@@ -94,6 +97,20 @@ def measure_peaks(device=None, l2_mib=48, l2_reps=20, ex2_iters=4096):
         t_l2 = timed(lambda: _lib.call("srf_probe_l2_read", buf.data_ptr(), n, l2_reps,
                                        sink.data_ptr(), stream))
         t_ex2 = timed(lambda: _lib.call("srf_probe_ex2", ex2_iters, sink.data_ptr(), stream))
+        ns = ctypes.c_int64(0)
+        _lib.call("srf_probe_smem_threads", ctypes.byref(ns))
+        ssink = torch.empty(ns.value, dtype=torch.float32, device=dev)
+        t_sm = timed(lambda: _lib.call("srf_probe_smem_read", smem_iters, ssink.data_ptr(),
+                                       stream))
+        t_at = timed(lambda: _lib.call("srf_probe_smem_atomic", atomic_iters, 0,
+                                       ssink.data_ptr(), stream))
+        t_ar = timed(lambda: _lib.call("srf_probe_smem_atomic", atomic_iters, 1,
+                                       ssink.data_ptr(), stream))
     l2_bytes = l2_reps * (n // 4) * 16
     return {"l2_gbs": l2_bytes / t_l2 / 1e9, "ex2_per_s": nt.value * 8 * ex2_iters / t_ex2,
-            "l2_buffer_mib": l2_mib, "method": "srf_probe_l2_read / srf_probe_ex2, CUDA events"}
+            "smem_gbs": ns.value * smem_iters * 16 / t_sm / 1e9,
+            "smem_atomic_per_s": ns.value * atomic_iters / t_at,
+            "smem_atomic_random_per_s": ns.value * atomic_iters / t_ar,
+            "l2_buffer_mib": l2_mib,
+            "method": "srf_probe_l2_read / srf_probe_ex2 / srf_probe_smem_read / "
+                      "srf_probe_smem_atomic, CUDA events"}

@@ -41,11 +41,12 @@ def mlem_update(image_prev, image_succ, efficiency_map):
 
 
 def mlem_update_normal(image_prev, image_succ, efficiency_map):
-    """x / effmap * bp (recon_step.py:52-53)."""
-    inv = torch.where(efficiency_map.data != 0, 1.0 / efficiency_map.data,
-                      torch.zeros_like(efficiency_map.data))
-    return mlem_update(image_prev, image_succ, Image(inv, efficiency_map.center,
-                                                     efficiency_map.size))
+    """x / effmap * bp (recon_step.py:52-53), with the reference's operation order: the
+    division first, then the product, so a voxel with zero efficiency gives inf or NaN
+    exactly as the reference does (``mlem_update`` with an inverted map is the path the
+    reconstruction uses; there zero-efficiency voxels carry effinv = 0)."""
+    out = image_prev.data / efficiency_map.data * image_succ.data
+    return Image(out, image_prev.center, image_prev.size)
 
 
 class ReconStep:

@@ -36,12 +36,14 @@ def set_scratch_limit(nbytes=0):
 
 
 def candidates(max_slab_slices):
-    """Settings worth trying: full and half-depth slabs, grid multipliers 1 and 2, the
-    spread-items slab kernel and the LOR-centric kernels."""
-    out = [(1, 0, 1), (1, 0, 2)]
+    """Settings worth trying: full and half-depth slabs, each with the library's automatic
+    grid multiplier (0: chosen per op and call size) and with multipliers 1 and 2 fixed,
+    the spread-items slab kernel and the LOR-centric kernels. The automatic choice comes
+    first, so a tie keeps it."""
+    out = [(1, 0, 0), (1, 0, 1), (1, 0, 2)]
     half = max(1, max_slab_slices // 2)
     if half < max_slab_slices:
-        out += [(1, half, 1), (1, half, 2)]
+        out += [(1, half, 0), (1, half, 1), (1, half, 2)]
     out += [(3, 0, 1), (2, 0, 1)]
     return out
 

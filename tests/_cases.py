@@ -10,7 +10,8 @@ import torch
 
 from oracle import preprocess_ref as P
 from srf_b200.scanner import RingScanner, tof_info
-from srf_b200.synthetic import generate_events, random_lors, standard_phantom
+from srf_b200.synthetic import (generate_events, large_fov_phantom, random_lors,
+                                standard_phantom)
 
 SCANNER = RingScanner(400.0, 400, 32, 3.2)
 KW_CONFIG = 6 * 4.0 / 2.35482005  # TOR FWHM 4 mm -> kernel_width 10.19 mm
@@ -89,3 +90,28 @@ def siddon_case(n=3000, seed=21, grid=(64, 64, 32), voxel=3.4, tof_res=530.0):
 def tof_params(tof_res, tof_bin_ps=40.0):
     b, s2 = tof_info(tof_res, tof_bin_ps)
     return float(np.float32(b)), float(np.float32(s2))
+
+
+# The large axial FOV configuration: R 390 mm, 600 crystals x 320 rings over 1 m
+# (3.125 mm pitch), 256x256x128 at 2.5 mm, 400 ps TOF.
+LARGE_SCANNER = RingScanner(390.0, 600, 320, 3.125)
+
+
+def large_case(n=3000, seed=71, n_box=800, tof_res=400.0):
+    """Events of the large-FOV multi-cylinder phantom on the 1 m scanner plus box events
+    (all three dominant-axis groups populated), preprocessed, with a noisy phantom image
+    at 256x256x128 / 2.5 mm."""
+    _, sig2 = tof_info(tof_res, 40.0)
+    ph = large_fov_phantom(half_length=LARGE_SCANNER.axial_length / 2)
+    ev = generate_events(n, LARGE_SCANNER, ph, seed, tof_sigma_mm=float(np.sqrt(sig2))).numpy()
+    if n_box:
+        ev = np.vstack([ev, box_events(n_box, seed + 1, half=(330.0, 330.0, 200.0),
+                                       tof_sigma=float(np.sqrt(sig2)))])
+    groups = P.recon_process(ev, tof_res)
+    grid, voxel = (256, 256, 128), 2.5
+    size = [g * voxel for g in grid]
+    img = ph.voxelize(grid, [0.0, 0.0, 0.0], size)
+    rng = np.random.default_rng(seed + 2)
+    img = (img + 0.25 * rng.random(img.shape, dtype=np.float32) + 0.05).astype(np.float32)
+    return dict(events=ev, groups=groups, image=img, grid=list(grid), center=[0.0, 0.0, 0.0],
+                size=size, tof_res=tof_res)

@@ -1,6 +1,7 @@
 """Generate tests/golden/reference_outputs.npz from the reference itself.
 
-Run in a container that has the SRF checkout (default /root/reference):
+Run in a container that has the SRF checkout (``--reference``, else $SRF_REFERENCE, else
+/root/reference):
 
     python tests/golden/make_golden.py [--reference PATH]
 
@@ -77,7 +78,8 @@ def load_reference_preprocessing(reference):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference",
+                    default=os.environ.get("SRF_REFERENCE", "/root/reference"))
     a = ap.parse_args(argv)
 
     from oracle import pyoracle as O

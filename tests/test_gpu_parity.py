@@ -497,6 +497,20 @@ def test_tor_projection_backprojection_chunked():
         assert K.rel_l2(b_, a) <= 1e-6
 
 
+@pytest.mark.parametrize("pname", ["tof530_kw10", "tof530_kw4_geo"])
+def test_tor_count_samples_match_oracle(tcase, pname):
+    """Per-LOR TOR work (non-zero-weight voxels, in-grid window voxels: the numerator of
+    the bench's roofline) equals the oracle's count for every axis group."""
+    kw, geo, _, _ = _tp(pname)
+    for axis in "xyz":
+        lors, _, g, c, s = K.tor_axis(tcase, axis)
+        slots, useful, _ = O.tor_counts(lors, g, c, s, kw, geo)
+        got = host(ops.tor_count_samples(cu(lors), g, c, s, kw, geo, layout="cn"))
+        assert useful.sum() > 0
+        np.testing.assert_array_equal(got[0].astype(np.int64), useful)
+        np.testing.assert_array_equal(got[1].astype(np.int64), slots)
+
+
 def test_siddon_count_samples_match_oracle():
     """Per-ray voxel visits of the Siddon walk equal the oracle's count (rays that miss
     the image, or start off the grid, visit none)."""

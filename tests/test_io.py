@@ -60,6 +60,23 @@ def test_stream_events_equals_one_upload(tmp_path):
 
 
 @pytest.mark.gpu
+def test_stream_events_chunk_survives_one_advance():
+    # a caller that pairs neighbouring chunks holds chunk k (uncloned) while it works on
+    # chunk k+1; both must still hold their own source rows
+    ev = _events(70_001, seed=9)
+    prev, prev_rows = None, None
+    bounds = io.chunk_bounds(ev.shape[0], 10_000)
+    for k, c in enumerate(io.stream_events(ev, chunk=10_000)):
+        s, e = bounds[k]
+        c.mul_(1.0)  # caller work on chunk k, queued on the current stream
+        if prev is not None:
+            np.testing.assert_array_equal(prev.cpu().numpy(), prev_rows)
+        np.testing.assert_array_equal(c.cpu().numpy(), ev[s:e])
+        prev, prev_rows = c, ev[s:e]
+    assert k == len(bounds) - 1
+
+
+@pytest.mark.gpu
 def test_load_split_equals_recon_process(tmp_path):
     from srf_b200 import preprocess as PP
     from tests import _cases as K

@@ -10,9 +10,30 @@ from srf_b200 import _lib, tuning
 
 
 def test_candidates():
-    assert tuning.candidates(16) == [(1, 0, 1), (1, 0, 2), (1, 8, 1), (1, 8, 2), (3, 0, 1),
-                                     (2, 0, 1)]
-    assert tuning.candidates(1) == [(1, 0, 1), (1, 0, 2), (3, 0, 1), (2, 0, 1)]
+    assert tuning.candidates(16) == [(1, 0, 0), (1, 0, 1), (1, 0, 2), (1, 8, 0), (1, 8, 1),
+                                     (1, 8, 2), (3, 0, 1), (2, 0, 1)]
+    assert tuning.candidates(1) == [(1, 0, 0), (1, 0, 1), (1, 0, 2), (3, 0, 1), (2, 0, 1)]
+
+
+def test_automatic_multiplier_competes_and_wins_ties(recorder):
+    # the automatic grid multiplier (0) is timed like any fixed one and, being first,
+    # is kept when a fixed multiplier only ties it
+    cands = tuning.candidates(6)
+    ms = {c: 5.0 for c in cands}
+    ms[(1, 0, 1)] = ms[(1, 0, 0)] = 4.0
+
+    def tune(key):
+        timer = FakeTimer(ms)
+
+        def step():
+            timer.current = recorder[-1]
+        return tuning.Autotuner(timer=timer).tune(key, step, cands)
+
+    best, timings = tune("k")
+    assert (1, 0, 0) in timings and best == (1, 0, 0)
+    ms[(1, 3, 0)] = 3.0  # the automatic multiplier at half-depth slabs, strictly faster
+    best, _ = tune("k2")
+    assert best == (1, 3, 0) and recorder[-1] == best
 
 
 def test_key_buckets():

@@ -75,3 +75,21 @@ def test_no_alloc_rejects_too_many_events():
                                        counts.data_ptr(), torch.cuda.current_stream().cuda_stream)
     assert st == 3  # SRF_ERR_UNSUPPORTED, nothing launched
     assert lib.srf_status_string(st) == b"unsupported parameters"
+
+
+def test_no_alloc_at_the_event_limit():
+    """A call with exactly SRF_RECON_PROCESS_NOALLOC_MAX_EVENTS events uses the whole
+    built-in scratch; it must still equal the workspace entry point, then a small call
+    right after it must too."""
+    lib = _lib.load()
+    big = K.box_events(MAX_EVENTS, 95)
+    small = K.box_events(5000, 96)
+    for events in (big, small):
+        ev = torch.as_tensor(events).cuda().contiguous()
+        ref_out, ref_counts = _with_workspace(lib, ev, 530.0)
+        got_out, got_counts = _no_alloc(lib, ev, 530.0)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(got_counts.cpu().numpy(), ref_counts.cpu().numpy())
+        assert int(ref_counts.sum()) == events.shape[0]
+        assert torch.equal(got_out, ref_out)
+        del ev, ref_out, got_out
