@@ -258,27 +258,20 @@ struct LorConst {
     bool all;        // map with a zero / non-finite divisor: every window voxel gets w/v
 };
 
-// Loads LOR t and derives its constants. Returns false when the LOR contributes
-// nothing (no crossing possible, or a back-projection value at/below 1e-7).
+// The per-LOR constants that do not depend on the op's values: direction, cut-off and
+// exponent slope, bounding-box half-extents, TOF centre and candidate slices. Returns
+// false when no crossing is possible (degenerate or non-finite LOR, bad frame id).
 template <int OP>
-__device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorConst &L) {
+__device__ __forceinline__ bool lor_geometry(const TorParams &p, int64_t t, LorConst &L) {
     L.all = false;
+    L.scale = p.tof_scale;
+    L.s_lo = 0;
+    L.s_hi = -1;
     if (!frame_ok(p, t)) return false;
     const int64_t o = t * p.stride;
     const float x1 = __ldg(p.x1 + o), y1 = __ldg(p.y1 + o), z1 = __ldg(p.z1 + o);
     const float x2 = __ldg(p.x2 + o), y2 = __ldg(p.y2 + o), z2 = __ldg(p.z2 + o);
     const float f = __ldg(p.f + o);
-    L.scale = p.tof_scale;
-    if (OP == kBack) {
-        const float v = __ldg(p.values + t);
-        if (!((double)v > 1e-7)) return false;  // tor.cu.cc:203
-        L.scale = __fdiv_rn(p.tof_scale, v);
-    } else if (OP == kMap) {
-        L.scale = __fdiv_rn(1.0f, __ldg(p.values + t));  // tor.cu.cc:239, no threshold
-        L.all = !(fabsf(L.scale) <= 3.0e38f);  // w/0 or w/NaN lands on every visited voxel
-    } else if (OP == kAdj) {
-        L.scale = p.tof_scale * __ldg(p.values + t);
-    }
     L.x1 = x1;
     L.y1 = y1;
     L.z1 = z1;
@@ -301,8 +294,8 @@ __device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorCo
         const float om_x = 1.0f - L.ux * L.ux, om_y = 1.0f - L.uy * L.uy;
         const float q = om_x - L.uy * L.uy;
         const float c = L.cut * 1.0001f + p.box_e;
-        const bool boxed = q > 1e-3f && !L.all && c < 3.0e38f;
-        // outside a box (nearly in-plane LOR, map LOR with a zero divisor): whole window
+        const bool boxed = q > 1e-3f && c < 3.0e38f;
+        // outside a box (nearly in-plane LOR): the whole window
         L.bxv = boxed ? sqrtf(c * om_y / q) * p.inv_x + (1.0f / 1024.0f) : 1.0e9f;
         L.byv = boxed ? sqrtf(c * om_x / q) * p.inv_y + (1.0f / 1024.0f) : 1.0e9f;
     }
@@ -321,16 +314,83 @@ __device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorCo
     return L.s_lo <= L.s_hi;
 }
 
-// Candidate slice range of LOR t from its endpoints only (cheap pre-filter).
-__device__ __forceinline__ bool lor_slices(const TorParams &p, int64_t t, int &s_lo,
-                                           int &s_hi) {
-    const int64_t o = t * p.stride;
-    const float z1 = __ldg(p.z1 + o), z2 = __ldg(p.z2 + o);
-    const float zlo = fminf(z1, z2), zhi = fmaxf(z1, z2);
-    if (!(z1 != z2 && zlo == zlo && zhi == zhi && fabsf(zhi - zlo) <= 3.0e38f)) return false;
-    s_lo = (int)fmaxf(floorf((zlo - p.slice0_f) / p.inter_z) - 2.0f, 0.0f);
-    s_hi = (int)fminf(ceilf((zhi - p.slice0_f) / p.inter_z) + 2.0f, (float)(p.gz - 1));
-    return s_lo <= s_hi;
+// The op's per-LOR output scale from its value (back-projection: tof_scale / v, dropped
+// at or below 1e-7, tor.cu.cc:203; map: 1 / v with no threshold, :239, where a zero or
+// non-finite divisor lands w/v on every visited voxel; adjoint: tof_scale * v). Returns
+// false when the LOR contributes nothing.
+template <int OP>
+__device__ __forceinline__ bool lor_value_scale(const TorParams &p, int64_t t, LorConst &L) {
+    if (OP == kBack) {
+        const float v = __ldg(p.values + t);
+        if (!((double)v > 1e-7)) return false;  // tor.cu.cc:203
+        L.scale = __fdiv_rn(p.tof_scale, v);
+    } else if (OP == kMap) {
+        L.scale = __fdiv_rn(1.0f, __ldg(p.values + t));  // tor.cu.cc:239, no threshold
+        L.all = !(fabsf(L.scale) <= 3.0e38f);  // w/0 or w/NaN lands on every visited voxel
+        if (L.all) L.bxv = L.byv = 1.0e9f;     // ... so the whole window is walked
+    } else if (OP == kAdj) {
+        L.scale = p.tof_scale * __ldg(p.values + t);
+    }
+    return true;
+}
+
+// Loads LOR t and derives its constants. Returns false when the LOR contributes
+// nothing (no crossing possible, or a back-projection value at/below 1e-7).
+template <int OP>
+__device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorConst &L) {
+    if (!lor_geometry<OP>(p, t, L)) return false;
+    return lor_value_scale<OP>(p, t, L);
+}
+
+// The binning pass stores each LOR's geometry once as a 64-byte record, so the slab
+// kernels take it with four 16-byte loads per segment instead of re-deriving it from the
+// ten columns in every slab the LOR meets:
+//   {x1, y1, z1, d0}, {d1, dz, ux, uy}, {cut, k1, bxv, byv}, {xc, yc, zc, slices}
+// with slices = s_lo | s_hi << 16, or -1 when the LOR contributes nothing.
+struct __align__(16) LorRec {
+    float4 a, b, c, d;
+};
+
+__device__ __forceinline__ LorRec make_rec(const LorConst &L, bool ok) {
+    LorRec r;
+    r.a = make_float4(L.x1, L.y1, L.z1, L.d0);
+    r.b = make_float4(L.d1, L.dz, L.ux, L.uy);
+    r.c = make_float4(L.cut, L.k1, L.bxv, L.byv);
+    r.d = make_float4(L.xc, L.yc, L.zc, __int_as_float(ok ? (L.s_lo | (L.s_hi << 16)) : -1));
+    return r;
+}
+
+__device__ __forceinline__ float4 ldg_f4(const float4 *q) {
+    float4 v;
+    asm("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(q));
+    return v;
+}
+
+// LOR t's geometry from its record; false when the LOR contributes nothing.
+__device__ __forceinline__ bool lor_rec_geometry(const LorRec *rec, int64_t t, LorConst &L) {
+    const float4 *q = reinterpret_cast<const float4 *>(rec + t);
+    const float4 d = ldg_f4(q + 3);
+    const int sl = __float_as_int(d.w);
+    const float4 a = ldg_f4(q), b = ldg_f4(q + 1), c = ldg_f4(q + 2);
+    L.x1 = a.x; L.y1 = a.y; L.z1 = a.z; L.d0 = a.w;
+    L.d1 = b.x; L.dz = b.y; L.ux = b.z; L.uy = b.w;
+    L.cut = c.x; L.k1 = c.y; L.bxv = c.z; L.byv = c.w;
+    L.xc = d.x; L.yc = d.y; L.zc = d.z;
+    L.s_lo = sl & 0xffff;
+    L.s_hi = sl >> 16;
+    L.all = false;
+    return sl >= 0;
+}
+
+// LOR t's constants from its record and the op's value (lor_prepare's result).
+template <int OP>
+__device__ __forceinline__ bool lor_load(const TorParams &p, const LorRec *rec, int64_t t,
+                                         LorConst &L) {
+    L.scale = p.tof_scale;
+    if (!lor_rec_geometry(rec, t, L)) return false;
+    return lor_value_scale<OP>(p, t, L);
 }
 
 // (int)(a / b) with a correctly rounded quotient, as the reference truncates it
@@ -601,27 +661,27 @@ struct SegPlan {
     int64_t *tile_offs;    // [ntiles * n_slabs]
     int64_t *slab_offs;    // [n_slabs + 1]
     int *seg;              // [capacity] LOR indices, slab-major
+    LorRec *rec;           // [n] per-LOR records written by seg_count
 };
 
 // Slab ids of LOR t (slice range k of its frame, row band b): id = k * nbands + b, with k
 // counted over frames. Calls g(id) for each. With row bands, the bands of slice range k
 // are those the LOR's window rows can reach in its slices there: the rows follow the
 // crossing point's y, which is monotonic in the slice, so the rows of the range's two end
-// slices, with two rows of margin and the window's extent, bound them.
+// slices, with two rows of margin and the window's extent, bound them. y1, z1, d1 = y2 - y1
+// and dz = z2 - z1 come from the LOR's record, so counting and filling agree bit for bit.
 template <bool kBand, typename G>
 __device__ __forceinline__ void lor_slab_ids(const TorParams &p, const SegPlan &sp, int64_t t,
-                                             int k_lo, int k_hi, int s_lo, int s_hi, G &&g) {
+                                             int k_lo, int k_hi, int s_lo, int s_hi, float y1,
+                                             float z1, float d1, float dz, G &&g) {
     if constexpr (!kBand) {
         for (int k = k_lo; k <= k_hi; k++) g(k);
         return;
     }
     const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
-    const int64_t o = t * p.stride;
-    const float y1 = __ldg(p.y1 + o), y2 = __ldg(p.y2 + o);
-    const float z1 = __ldg(p.z1 + o), z2 = __ldg(p.z2 + o);
     auto y_at = [&](int s) {
-        const float r = (p.slice0_f + (float)s * p.inter_z - z1) / (z2 - z1);
-        return fmaf(y2 - y1, fminf(fmaxf(r, 0.0f), 1.0f), y1);
+        const float r = (p.slice0_f + (float)s * p.inter_z - z1) / dz;
+        return fmaf(d1, fminf(fmaxf(r, 0.0f), 1.0f), y1);
     };
     for (int k = k_lo; k <= k_hi; k++) {
         const int first = (k - f0) * sp.nsl;
@@ -665,14 +725,21 @@ __global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams 
     for (int it = 0; it < kSegItems; it++) {
         const int64_t t = base + (int64_t)it * kSegThreads + threadIdx.x;
         if (t >= p.n) break;
-        int s_lo, s_hi, packed = -1;
-        bool ok = frame_ok(p, t) && lor_slices(p, t, s_lo, s_hi);
+        int packed = -1;
+        LorConst L;
+        bool ok = lor_geometry<OP>(p, t, L);
+        const LorRec r = make_rec(L, ok);
+        float4 *q = reinterpret_cast<float4 *>(sp.rec + t);
+        q[0] = r.a;
+        q[1] = r.b;
+        q[2] = r.c;
+        q[3] = r.d;
         if (ok && OP == kBack) ok = (double)__ldg(p.values + t) > 1e-7;  // tor.cu.cc:203
         if (ok) {
             const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
-            const int k_lo = f0 + s_lo / sp.nsl, k_hi = f0 + s_hi / sp.nsl;
+            const int k_lo = f0 + L.s_lo / sp.nsl, k_hi = f0 + L.s_hi / sp.nsl;
             packed = k_lo | (k_hi << 16);
-            lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi,
+            lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, L.s_lo, L.s_hi, L.y1, L.z1, L.d1, L.dz,
                                 [&](int id) { atomicAdd(&hist[id], 1); });
         }
         sp.range[t] = packed;
@@ -743,47 +810,24 @@ __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p
         if (packed < 0) continue;
         const int k_lo = packed & 0xffff, k_hi = packed >> 16;
         int s_lo = 0, s_hi = p.gz - 1;
-        if (kBand) lor_slices(p, t, s_lo, s_hi);  // same range as seg_count's
-        lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi, [&](int id) {
+        float y1 = 0.f, z1 = 0.f, d1 = 0.f, dz = 1.f;
+        if (kBand) {  // the values seg_count used, from the LOR's record
+            const float4 *q = reinterpret_cast<const float4 *>(sp.rec + t);
+            const float4 a = q[0], b = q[1], d = q[3];
+            const int sl = __float_as_int(d.w);
+            s_lo = sl & 0xffff;
+            s_hi = sl >> 16;
+            y1 = a.y;
+            z1 = a.z;
+            d1 = b.x;
+            dz = b.y;
+        }
+        lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi, y1, z1, d1, dz, [&](int id) {
             const int pos = warp_increment(cursor, id);
             sp.seg[sp.slab_offs[id] + sp.tile_offs[(int64_t)blockIdx.x * sp.n_slabs + id] + pos] =
                 (int)t;
         });
     }
-}
-
-// Persistent pass over the slab-major segment list (all TOR ops but the count).
-// Each warp takes 32 segments, expands them into (segment, slice) items and hands out
-// 32 items per round, so every lane walks one slice of one LOR; the LOR constants come
-// from the segment's lane by shuffle. Scatter ops accumulate into the slab with shared
-// atomics and flush once per slab; the projection gathers from the slab (loaded from
-// the image) and adds each LOR's partial sum, reduced across the warp, to its output.
-template <int OP>
-__device__ __forceinline__ LorConst shfl_lor(const LorConst &L, int src) {
-    LorConst M;
-    M.x1 = __shfl_sync(0xffffffffu, L.x1, src);
-    M.y1 = __shfl_sync(0xffffffffu, L.y1, src);
-    M.z1 = __shfl_sync(0xffffffffu, L.z1, src);
-    M.d0 = __shfl_sync(0xffffffffu, L.d0, src);
-    M.d1 = __shfl_sync(0xffffffffu, L.d1, src);
-    M.dz = __shfl_sync(0xffffffffu, L.dz, src);
-    M.ux = __shfl_sync(0xffffffffu, L.ux, src);
-    M.uy = __shfl_sync(0xffffffffu, L.uy, src);
-    M.cut = __shfl_sync(0xffffffffu, L.cut, src);
-    M.k1 = __shfl_sync(0xffffffffu, L.k1, src);
-    M.bxv = __shfl_sync(0xffffffffu, L.bxv, src);
-    M.byv = __shfl_sync(0xffffffffu, L.byv, src);
-    if (OP != kMap) {
-        M.xc = __shfl_sync(0xffffffffu, L.xc, src);
-        M.yc = __shfl_sync(0xffffffffu, L.yc, src);
-        M.zc = __shfl_sync(0xffffffffu, L.zc, src);
-    } else {
-        M.xc = M.yc = M.zc = 0.0f;
-    }
-    M.scale = __shfl_sync(0xffffffffu, L.scale, src);
-    M.all = OP == kMap ? (bool)__shfl_sync(0xffffffffu, (int)L.all, src) : false;
-    M.s_lo = M.s_hi = 0;
-    return M;
 }
 
 // Shared-memory slab layout. Every slice of the slab has pad = P - 1 zero rows and
@@ -805,9 +849,13 @@ __host__ __device__ __forceinline__ int slab_floats(int nsl, int gx, int gy, int
     return nsl * slab_slice_stride(gx, gy, pad) + slab_origin(gx, pad);
 }
 
+// Persistent pass over the slab-major segment list (all TOR ops but the count). Scatter
+// ops accumulate into the slab with shared atomics and flush once per slab; the
+// projection gathers from the slab (loaded from the image) and adds each LOR's partial
+// sum to its output.
 // kExpand: the (LOR, slice) items of a warp's 32 segments are spread over its lanes, 32
-// at a time (one item per lane, LOR constants shuffled to it); otherwise each lane walks
-// its own segment's slices.
+// at a time (one item per lane, the LOR's constants read from its record); otherwise
+// each lane walks its own segment's slices.
 // kBand: the slabs are bands of rows (sp.nbands > 1), so rows are limited to the band.
 template <int OP, int P, bool kExpand, bool kBand>
 __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorParams p, SegPlan sp) {
@@ -870,7 +918,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
             int a = 0, cnt = 0, t = -1;
             if (q < end) {
                 t = sp.seg[q];
-                if (lor_prepare<OP>(p, t, L)) {
+                if (lor_load<OP>(p, sp.rec, t, L)) {
                     a = max(L.s_lo, S0);
                     cnt = max(0, min(L.s_hi, S1 - 1) - a + 1);
                 }
@@ -912,10 +960,20 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                 const bool valid = item < n_items;
                 const int o = valid ? (int)owner_tab[warp][lane] : 0;
                 __syncwarp();
-                const LorConst M = shfl_lor<OP>(L, o);
                 const int a_o = __shfl_sync(0xffffffffu, a, o);
                 const int excl_o = __shfl_sync(0xffffffffu, excl, o);
                 const int t_o = __shfl_sync(0xffffffffu, t, o);
+                // the item's LOR from its record (the lanes of one LOR read the same 64
+                // bytes, served once by L1), its value scale from the owning lane
+                LorConst M;
+                const float scale_o = __shfl_sync(0xffffffffu, L.scale, o);
+                const bool all_o = OP == kMap && __shfl_sync(0xffffffffu, (int)L.all, o);
+                if (valid) {
+                    lor_rec_geometry(sp.rec, t_o, M);
+                    M.scale = scale_o;
+                    M.all = all_o;
+                    if (all_o) M.bxv = M.byv = 1.0e9f;
+                }
                 float partial = 0.0f;
                 if (valid) {
                     const int s = a_o + (item - excl_o);
@@ -1134,11 +1192,12 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
     SegPlan sp{};
     if (!slab_geometry(p, P - 1, sp)) return -1;
     // The segment list is sized for the worst case (every LOR in every slab of its frame);
-    // LORs are taken in chunks small enough that this stays within the scratch budget
-    // (at least one 4096-LOR tile per chunk).
+    // with each LOR's record and slab range, LORs are taken in chunks small enough that
+    // this stays within the scratch budget (at least one 4096-LOR tile per chunk).
     const int64_t max_slabs_per_lor = (int64_t)sp.slabs_pf * sp.nbands;
     const size_t budget = (size_t)g_seg_scratch_bytes.load(std::memory_order_relaxed);
-    int64_t chunk = (int64_t)(budget / (sizeof(int) * (size_t)max_slabs_per_lor));
+    int64_t chunk = (int64_t)(budget / (sizeof(int) * (size_t)max_slabs_per_lor +
+                                        sizeof(LorRec) + sizeof(int)));
     chunk = std::max<int64_t>(kSegTile, chunk / kSegTile * kSegTile);
     chunk = std::min<int64_t>(chunk, p.n);
     sp.ntiles = (int)((chunk + kSegTile - 1) / kSegTile);
@@ -1150,18 +1209,21 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
     const size_t b_offs = al(sizeof(int64_t) * (size_t)sp.ntiles * sp.n_slabs);
     const size_t b_slab = al(sizeof(int64_t) * (2 * sp.n_slabs + 1));
     const size_t b_seg = al(sizeof(int) * cap);
+    const size_t b_rec = al(sizeof(LorRec) * chunk);
     char *ws = nullptr;
-    cudaError_t e = scratch_alloc((void **)&ws, b_range + b_counts + b_offs + b_slab + b_seg,
-                                  stream);
+    cudaError_t e = scratch_alloc((void **)&ws,
+                                  b_rec + b_range + b_counts + b_offs + b_slab + b_seg, stream);
     if (e != cudaSuccess) {
         set_cuda_error(e);
         return SRF_ERR_CUDA;
     }
-    sp.range = reinterpret_cast<int *>(ws);
-    sp.tile_counts = reinterpret_cast<int *>(ws + b_range);
-    sp.tile_offs = reinterpret_cast<int64_t *>(ws + b_range + b_counts);
-    sp.slab_offs = reinterpret_cast<int64_t *>(ws + b_range + b_counts + b_offs);
-    sp.seg = reinterpret_cast<int *>(ws + b_range + b_counts + b_offs + b_slab);
+    sp.rec = reinterpret_cast<LorRec *>(ws);
+    char *w2 = ws + b_rec;
+    sp.range = reinterpret_cast<int *>(w2);
+    sp.tile_counts = reinterpret_cast<int *>(w2 + b_range);
+    sp.tile_offs = reinterpret_cast<int64_t *>(w2 + b_range + b_counts);
+    sp.slab_offs = reinterpret_cast<int64_t *>(w2 + b_range + b_counts + b_offs);
+    sp.seg = reinterpret_cast<int *>(w2 + b_range + b_counts + b_offs + b_slab);
 
     const bool band = sp.nbands > 1;
     void (*kern)(const TorParams, SegPlan) = nullptr;
