@@ -181,6 +181,12 @@ int srf_tor_backproject_adjoint_batched(const float *x1, const float *y1, const 
  * whole-slice slabs, else 1). */
 int srf_tor_set_tuning(int path, int slab_slices, int grid_mult);
 
+/* No counterpart in the reference: the Siddon kernel family. path 0: automatic (the
+ * shared-memory z-slab kernels wherever a z-slice of the image fits in shared memory and
+ * the image has at most 32 slabs; the count op always uses path 2); 1: the same; 2: one
+ * thread per ray, gathers from L2 and global atomics. Process-wide. */
+int srf_siddon_set_tuning(int path);
+
 /* No counterpart in the reference: upper bound, in bytes, of the per-slab LOR lists the
  * slab kernels build per call (0 = the default, 1 GiB). The lists are sized for the worst
  * case, 4 bytes x LORs x slabs per frame; a call with more LORs than fit is processed in

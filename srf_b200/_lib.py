@@ -51,6 +51,7 @@ SIGNATURES = {
                                                          _f, _f, _f, _p, _i64, _i64, _int, _p],
                                             _int),
     "srf_tor_set_tuning": ([_int, _int, _int], _int),
+    "srf_siddon_set_tuning": ([_int], _int),
     "srf_tor_set_scratch_limit": ([_i64], _int),
     "srf_tor_count_samples": ([_p] * 7 + [_int, _p, _p, _p, _f, _p, _i64, _i64, _p], _int),
     "srf_siddon_count_samples": ([_p] * 6 + [_p, _p, _p, _p, _i64, _i64, _p], _int),

@@ -254,6 +254,7 @@ struct LorConst {
     float bxv, byv;  // bounding-box half-extents in voxels (margin included)
     float xc, yc, zc;
     float scale;
+    float k0s;       // back-projection: log2(scale), folded into the exponent (else 0)
     int s_lo, s_hi;  // candidate slices (a superset; each is tested exactly)
     bool all;        // map with a zero / non-finite divisor: every window voxel gets w/v
 };
@@ -265,6 +266,7 @@ template <int OP>
 __device__ __forceinline__ bool lor_geometry(const TorParams &p, int64_t t, LorConst &L) {
     L.all = false;
     L.scale = p.tof_scale;
+    L.k0s = 0.0f;
     L.s_lo = 0;
     L.s_hi = -1;
     if (!frame_ok(p, t)) return false;
@@ -324,6 +326,12 @@ __device__ __forceinline__ bool lor_value_scale(const TorParams &p, int64_t t, L
         const float v = __ldg(p.values + t);
         if (!((double)v > 1e-7)) return false;  // tor.cu.cc:203
         L.scale = __fdiv_rn(p.tof_scale, v);
+        // w * scale = 2^(log2 w + log2 scale): the scale joins the exponent (one add per
+        // slice instead of one multiply per voxel). scale = m 2^e with m in [0.5, 1):
+        // log2 m from the hardware approximation (absolute error ~2^-22) plus e exactly.
+        int e;
+        const float m = frexpf(L.scale, &e);
+        L.k0s = (float)e + __log2f(m);
     } else if (OP == kMap) {
         L.scale = __fdiv_rn(1.0f, __ldg(p.values + t));  // tor.cu.cc:239, no threshold
         L.all = !(fabsf(L.scale) <= 3.0e38f);  // w/0 or w/NaN lands on every visited voxel
@@ -381,6 +389,7 @@ __device__ __forceinline__ bool lor_rec_geometry(const LorRec *rec, int64_t t, L
     L.s_lo = sl & 0xffff;
     L.s_hi = sl >> 16;
     L.all = false;
+    L.k0s = 0.0f;
     return sl >= 0;
 }
 
@@ -501,11 +510,11 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
         wx = mx;
         wy = my;
     }
-    float k0 = 0.0f;
+    float k0 = OP == kBack ? L.k0s : 0.0f;
     if (OP != kMap && OP != kCount && p.tof_on) {
         const float ax = __fsub_rn(L.xc, cx), ay = __fsub_rn(L.yc, cy), az = __fsub_rn(L.zc, sz);
         const float a2 = __fmaf_rn(az, az, __fmaf_rn(ax, ax, __fmul_rn(ay, ay)));
-        k0 = -a2 * p.a_coef;
+        k0 = fmaf(-a2, p.a_coef, k0);
     }
     float dxs[P];
     const float fx0 = (float)xlo;
@@ -535,23 +544,24 @@ __device__ __forceinline__ int slice_visit(const TorParams &p, const LorConst &L
                     return L.cut;
                 }
             };
+            // fj = ylo + j + 0.5 (a half-integer: adding 1 per row is exact)
             if (OP == kProj) {
                 with_width<P>(wx, [&](auto W) {
-                    for (int j = 0; j < wy; j++) {
+                    float fj = fy0;
+                    for (int j = 0; j < wy; j++, fj += 1.0f) {
                         bool all;
                         const float cut = row_cut(j, all);
-                        const float dy =
-                            __fsub_rn(cy, __fmaf_rn(p.inter_y, fy0 + (float)j, p.b_bound));
+                        const float dy = __fsub_rn(cy, __fmaf_rn(p.inter_y, fj, p.b_bound));
                         row_slots<OP, decltype(W)::value>(L, cut, all, dxs, dy, k0, xlo, ylo + j,
                                                           f);
                     }
                 });
             } else {
-                for (int j = 0; j < wy; j++) {
+                float fj = fy0;
+                for (int j = 0; j < wy; j++, fj += 1.0f) {
                     bool all;
                     const float cut = row_cut(j, all);
-                    const float dy =
-                        __fsub_rn(cy, __fmaf_rn(p.inter_y, fy0 + (float)j, p.b_bound));
+                    const float dy = __fsub_rn(cy, __fmaf_rn(p.inter_y, fj, p.b_bound));
                     with_width<P>(wx, [&](auto W) {
                         row_slots<OP, decltype(W)::value>(L, cut, all, dxs, dy, k0, xlo, ylo + j,
                                                           f);
@@ -603,7 +613,8 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
                     } else if (OP == kProj) {
                         if (use) acc = fmaf(w, __ldg(p.image_in + idx), acc);
                     } else {
-                        if (use) atomicAdd(p.image_out + idx, w * L.scale);
+                        // back-projection: the scale is in w's exponent already
+                        if (use) atomicAdd(p.image_out + idx, OP == kBack ? w : w * L.scale);
                     }
                 });
             }
@@ -937,7 +948,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                     } else {
                         slice_visit<OP, P, true, kBand>(p, L, s, R0, R1,
                                                  [&](int ix, int iy, float w, bool use) {
-                            if (use) atomicAdd(&sb[(iy - R0) * rs + ix], w * L.scale);
+                            if (use)
+                                atomicAdd(&sb[(iy - R0) * rs + ix], OP == kBack ? w : w * L.scale);
                         });
                     }
                 }
@@ -967,10 +979,12 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                 // bytes, served once by L1), its value scale from the owning lane
                 LorConst M;
                 const float scale_o = __shfl_sync(0xffffffffu, L.scale, o);
+                const float k0s_o = __shfl_sync(0xffffffffu, L.k0s, o);
                 const bool all_o = OP == kMap && __shfl_sync(0xffffffffu, (int)L.all, o);
                 if (valid) {
                     lor_rec_geometry(sp.rec, t_o, M);
                     M.scale = scale_o;
+                    M.k0s = k0s_o;
                     M.all = all_o;
                     if (all_o) M.bxv = M.byv = 1.0e9f;
                 }
@@ -989,7 +1003,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                     } else {
                         slice_visit<OP, P, true, kBand>(p, M, s, R0, R1,
                                                  [&](int ix, int iy, float w, bool use) {
-                            if (use) atomicAdd(&sb[(iy - R0) * rs + ix], w * M.scale);
+                            if (use)
+                                atomicAdd(&sb[(iy - R0) * rs + ix], OP == kBack ? w : w * M.scale);
                         });
                     }
                 }
