@@ -288,8 +288,16 @@ __global__ void __launch_bounds__(256) sid_bin_kernel(const SiddonParams p, SidP
         int k_lo = 0, k_hi = -1;
         Ray R;
         if (t < p.n && ray_setup<OP>(p, t, R)) {
-            // z at the exit point, in the box-corner frame
-            const float zt = fmaf(R.tmax, R.dirz, R.z0);
+            // The walk runs to the grid's edge, not to the ray's end point (it stops only
+            // when a voxel counter runs out, siddon.cu.cc:302), so its last z is where
+            // the first axis leaves the grid: t_end (from the entry point) = min over the
+            // moving axes of next_t + (in_buf - 1) delta_t; z in the box-corner frame.
+            float t_end = INFINITY;
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+                if (R.step[a] != 0)
+                    t_end = fminf(t_end, fmaf((float)(R.in_buf[a] - 1), R.delta_t[a], R.next_t[a]));
+            const float zt = fmaf(R.tmin + t_end, R.dirz, R.z0);
             const float fz = fminf(fmaxf(floorf(zt / p.v_res[2]), -4.0f), (float)p.g[2] + 4.0f);
             const int izt = (int)fz;
             const int lo = max(0, min(R.pos[2], izt) - 2);
