@@ -95,7 +95,8 @@ def parse_args(argv=None):
                     help="skip the config variants of the same step (the reference preset "
                          "kernel_width 4.0; the geometric sigma2 factor on)")
     ap.add_argument("--tuning", default=None,
-                    help="PATH,SLAB_SLICES,GRID_MULT for srf_tor_set_tuning (default: the "
+                    help="PATH,SLAB_SLICES,GRID_MULT for srf_tor_set_tuning, or PATH for "
+                         "srf_siddon_set_tuning with --workload siddon64 (default: the "
                          "library's automatic choice)")
     return ap.parse_args(argv)
 
@@ -595,6 +596,52 @@ def cpu_baseline(groups_host, wl, tof_bin, tof_sigma2, image_np, target_s):
                       f"{t1:.1f} s wall"}
 
 
+def siddon_roofline(kern, steps, n_rays, visits, image_bytes, hbm_peak, peak_src, workload):
+    """The Siddon line's ``roofline`` object for the dominant op, with the bound of the
+    survey's measurement section, T* = max(B_HBM / HBM peak, B / L2 peak, exps / SFU
+    peak): B_HBM = the 28 B ray record and its 4 B value or output once per ray, plus the
+    image once (projection) or read-modify-written once (back-projection); B = B_HBM plus
+    4 B (projection) or 8 B (back-projection) per visited voxel, served by the L2 where
+    the image stays; no exps with TOF off. ``achieved`` = the binding term's bytes per
+    launch / the launch's mean CUDA-event time."""
+    from srf_b200 import profiling
+    if not kern:
+        return None
+    dom = max(kern, key=lambda k: kern[k]["total_ms"])
+    back = dom != "srf_siddon_projection"
+    b_hbm = n_rays * 32 + image_bytes * (2 if back else 1)
+    b_all = b_hbm + visits * (8 if back else 4)
+    probe = profiling.measure_peaks()
+    t_meas = kern[dom]["total_ms"] / steps / 1e3
+    terms = {"hbm": b_hbm / (hbm_peak * 1e9), "l2": b_all / (probe["l2_gbs"] * 1e9), "sfu": 0.0}
+    term = max(terms, key=terms.get)
+    per_launch = steps / max(kern[dom]["launches"], 1)
+    mean_s = kern[dom]["mean_ms"] / 1e3
+    nbytes = (b_all if term == "l2" else b_hbm) * per_launch
+    peak = probe["l2_gbs"] if term == "l2" else hbm_peak
+    achieved = nbytes / mean_s / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    if os.path.exists(prof):
+        traffic = json.load(open(prof)).get(workload, {}).get(dom)
+    return {"kernel": dom, "bound": term, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic,
+            "peak_source": f"{peak_src} hbm_gbs (burst copy) for the HBM term; L2 peak from "
+                           "the library's probe in this run",
+            "b_hbm_per_launch": b_hbm * per_launch, "algorithmic_bytes_per_launch": b_all * per_launch,
+            "visited_voxels_per_step": visits,
+            "components": {"hbm": {"ms": terms["hbm"] * 1e3, "frac": terms["hbm"] / t_meas,
+                                   "bytes": b_hbm, "peak_gbs": hbm_peak},
+                           "l2": {"ms": terms["l2"] * 1e3, "frac": terms["l2"] / t_meas,
+                                  "bytes": b_all, "peak_gbs": probe["l2_gbs"]},
+                           "sfu": {"ms": 0.0, "frac": 0.0, "exps": 0},
+                           "bound_term": term, "bound_ms": terms[term] * 1e3,
+                           "measured_ms": t_meas * 1e3, "frac_of_bound": terms[term] / t_meas},
+            "kernel_ms": {k: {"launches": v["launches"], "mean_ms": v["mean_ms"],
+                              "share": v["total_ms"] / sum(x["total_ms"] for x in kern.values())}
+                          for k, v in kern.items()}}
+
+
 def run_siddon(args):
     """Plain non-TOF Siddon (the CPU-runnable configuration): R 400 mm, 400 x 32
     crystals, 64x64x32 image at 3.4 mm, 1M seeded events from the cylinder phantom,
@@ -610,6 +657,9 @@ def run_siddon(args):
     from srf_b200.preprocess import initial_image
     world, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
+    if args.tuning:
+        from srf_b200 import tuning
+        tuning.set_siddon_tuning(int(args.tuning.split(",")[0]))
     wl = S.siddon_64()
     n = args.events or wl.n_events
     phantom = S.standard_phantom(half_length=wl.scanner.axial_length / 2)
@@ -696,30 +746,11 @@ def run_siddon(args):
     torch.cuda.synchronize()
     osem_ms = s0.elapsed_time(s1) / wl.iterations
 
-    # roofline: per LOR 28 B record + 4 B out/value + 4 B (8 B) per visited voxel
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    alg = {"srf_siddon_projection": n * 32 + 4 * visits,
-           "srf_siddon_backprojection": n * 32 + 8 * visits}
-    roof = None
-    if kern:
-        dom = max(kern, key=lambda k: kern[k]["total_ms"])
-        per_launch = alg.get(dom, 0) * args.steps / max(kern[dom]["launches"], 1)
-        achieved = per_launch / (kern[dom]["mean_ms"] / 1e3) / 1e9
-        probe = profiling.measure_peaks()
-        t_meas = kern[dom]["total_ms"] / args.steps / 1e3
-        t_l2 = alg.get(dom, 0) / (probe["l2_gbs"] * 1e9)
-        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
-                "peak_source": "measured hbm_gbs (burst copy)" if "hbm_gbs" in peaks
-                else "fallback hbm_gbs",
-                "algorithmic_bytes_per_launch": per_launch, "visited_voxels_per_step": visits,
-                "components": {"hbm": {"frac": achieved / hbm_peak},
-                               "l2": {"frac": t_l2 / t_meas, "peak_gbs": probe["l2_gbs"]},
-                               "sfu": {"frac": 0.0, "exps": 0}},
-                "kernel_ms": {k: {"launches": v["launches"], "mean_ms": v["mean_ms"]}
-                              for k, v in kern.items()}}
+    roof = siddon_roofline(kern, args.steps, n, visits, int(np.prod(wl.grid)) * 4, hbm_peak,
+                           "measured" if "hbm_gbs" in peaks else "fallback", wl.name)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -736,7 +767,8 @@ def run_siddon(args):
                 "config": {"workload": wl.name, "grid": list(wl.grid), "voxel_mm": wl.voxel,
                            "events_per_rank": int(n), "tof_sigma2": 1.0e6,
                            "parallelism": f"events sharded, {world} rank(s)",
-                           "l2": "image (0.5 MB) L2-resident; LOR records 28 MB per rank"},
+                           "l2": "image (0.5 MB) L2-resident; LOR records 28 MB per rank",
+                           "tuning": args.tuning or "automatic"},
                 "osem_iteration_ms": osem_ms,
                 "osem": {"subsets": wl.subsets, "iterations_timed": wl.iterations,
                          "effmap_lors": 10_000_000},

@@ -182,9 +182,9 @@ int srf_tor_backproject_adjoint_batched(const float *x1, const float *y1, const 
 int srf_tor_set_tuning(int path, int slab_slices, int grid_mult);
 
 /* No counterpart in the reference: the Siddon kernel family. path 0: automatic (the
- * shared-memory z-slab kernels wherever a z-slice of the image fits in shared memory and
- * the image has at most 32 slabs; the count op always uses path 2); 1: the same; 2: one
- * thread per ray, gathers from L2 and global atomics. Process-wide. */
+ * scatter ops reduce four consecutive voxels at a time wherever the image is 16-byte
+ * aligned and its voxel count is a multiple of 4); 1: one atomic per voxel. The projection
+ * gathers one voxel at a time either way. Process-wide. */
 int srf_siddon_set_tuning(int path);
 
 /* No counterpart in the reference: upper bound, in bytes, of the per-slab LOR lists the

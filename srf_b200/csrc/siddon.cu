@@ -11,7 +11,8 @@
 // and copies the geometry device-to-host first). The walk state (next boundary,
 // step, voxel counters) is evaluated with the same float operations as the reference,
 // so each ray visits the same voxels with the same chord lengths; the TOF weight of a
-// voxel uses float arithmetic for the Gaussian itself.
+// voxel uses float arithmetic for the Gaussian itself. The image is read and reduced
+// into four consecutive voxels at a time where a ray's run allows (siddon_kernel).
 
 #include <algorithm>
 #include <atomic>
@@ -90,18 +91,19 @@ __device__ __forceinline__ void setup_axis(float p0, float dir, float min_t, flo
 
 // One ray's walk state after SetupRayCast (siddon.cu.cc:261-284) and its weights.
 struct Ray {
-    int pos[3], step[3], in_buf[3];
-    float next_t[3], delta_t[3];
-    int boffs, stillin;
-    int zdir;             // +1 / -1 / 0: direction of the walk along z
+    float nt0, nt1, nt2;  // next boundary along x, y, z (from the entry point)
+    float dt0, dt1, dt2;  // boundary spacing along x, y, z
+    int in0, in1, in2;    // voxels left along x, y, z
+    int s1, s2;           // index steps of a y and a z move (an x move steps by +-1)
+    int s0;
+    int boffs;            // index of the current voxel
     float weight, t_tof;  // 1/L^2 (siddon.cu.cc:459), TOF position (:460)
-    float tmin, tmax, z0, dirz;
     float oscale;         // back-projection / map: 1/value; adjoint: value
 };
 
 // CreateRay, IsThroughImage and SetupRayCast of ray t. Returns false when the ray
 // contributes nothing (misses the box, value at/below 0 for back-projection and map,
-// start voxel off the grid).
+// start voxel off the grid, a voxel counter already at 0).
 template <int OP>
 __device__ __forceinline__ bool ray_setup(const SiddonParams &p, int64_t t, Ray &R) {
     const int64_t o = t * p.stride;
@@ -132,20 +134,25 @@ __device__ __forceinline__ bool ray_setup(const SiddonParams &p, int64_t t, Ray 
     if (!(through && tmin < tmax)) return false;
 
     // SetupRayCast (siddon.cu.cc:261-284).
+    int pos[3], step[3], in_buf[3];
+    float next_t[3], delta_t[3];
 #pragma unroll
     for (int k = 0; k < 3; k++)
-        setup_axis(__fsub_rn(start[k], p.corner[k]), dir[k], tmin, p.v_res[k], p.g[k], R.pos[k],
-                   R.next_t[k], R.delta_t[k], R.step[k], R.in_buf[k]);
-    R.zdir = R.step[2];
-    R.step[1] *= p.g[0];
-    R.step[2] *= p.g[0] * p.g[1];
-    R.boffs = R.pos[0] + p.g[0] * (R.pos[1] + p.g[1] * R.pos[2]);
-    R.stillin = R.in_buf[0] * R.in_buf[1] * R.in_buf[2];
+        setup_axis(__fsub_rn(start[k], p.corner[k]), dir[k], tmin, p.v_res[k], p.g[k], pos[k],
+                   next_t[k], delta_t[k], step[k], in_buf[k]);
     // A start voxel off the grid would make the reference read outside the image; such
     // a ray contributes nothing here.
-    if (!(R.pos[0] >= 0 && R.pos[0] < p.g[0] && R.pos[1] >= 0 && R.pos[1] < p.g[1] &&
-          R.pos[2] >= 0 && R.pos[2] < p.g[2]))
+    if (!(pos[0] >= 0 && pos[0] < p.g[0] && pos[1] >= 0 && pos[1] < p.g[1] && pos[2] >= 0 &&
+          pos[2] < p.g[2]))
         return false;
+    if (in_buf[0] * in_buf[1] * in_buf[2] == 0) return false;  // stillin = 0: no voxel
+    R.nt0 = next_t[0]; R.nt1 = next_t[1]; R.nt2 = next_t[2];
+    R.dt0 = delta_t[0]; R.dt1 = delta_t[1]; R.dt2 = delta_t[2];
+    R.in0 = in_buf[0]; R.in1 = in_buf[1]; R.in2 = in_buf[2];
+    R.s0 = step[0];
+    R.s1 = step[1] * p.g[0];
+    R.s2 = step[2] * p.g[0] * p.g[1];
+    R.boffs = pos[0] + p.g[0] * (pos[1] + p.g[1] * pos[2]);
 
     // weight (siddon.cu.cc:459, :514 and :557) and TOF position (:460).
     R.weight = (OP == kMap) ? __fdiv_rn(1.0f, __fmul_rn(length, length))
@@ -155,231 +162,110 @@ __device__ __forceinline__ bool ray_setup(const SiddonParams &p, int64_t t, Ray 
         R.t_tof = __double2float_rn((double)length * 0.5 - (double)tmin -
                                     (double)__ldg(p.tof + o));
     R.oscale = (OP == kBack || OP == kMap) ? __fdiv_rn(1.0f, vscale) : vscale;
-    R.tmin = tmin;
-    R.tmax = tmax;
-    R.z0 = __fsub_rn(z1, p.corner[2]);
-    R.dirz = dir[2];
-    return R.stillin != 0;
+    return true;
 }
 
-// RayTracing / BackRayTracing / Map (siddon.cu.cc:293-415): visits the ray's voxels in
-// order; f(mi, iz, val, use) gets the voxel index, its z index, the weight * chord length
-// [* TOF] and the reference's TOF cut decision, and returns false to end the walk early.
-// Returns the number of voxels visited.
-template <int OP, typename F>
-__device__ __forceinline__ int ray_walk(const SiddonParams &p, Ray &R, F &&f) {
-    const float sqrt2pi = 2.5066282746310002f;
-    const bool tof = (OP != kMap && OP != kCount) && p.tof_on;
-    float last_t = 0.0f;
-    int iz = R.pos[2];
-    int n_visits = 0;
-    int stillin = R.stillin;
-    while (stillin) {
-        // argmin with the reference's tie order (siddon.cu.cc:305)
-        const int i = (R.next_t[0] <= R.next_t[1]) ? ((R.next_t[0] <= R.next_t[2]) ? 0 : 2)
-                                                   : ((R.next_t[1] <= R.next_t[2]) ? 1 : 2);
-        const float nt = i == 0 ? R.next_t[0] : (i == 1 ? R.next_t[1] : R.next_t[2]);
-        const float l_len = __fsub_rn(nt, last_t);
-        float val;  // weight * l_len * [TOF] for this voxel
-        bool use = true;
-        if (tof) {
-            const float tt = __fmaf_rn(-0.5f, __fadd_rn(nt, last_t), R.t_tof);
-            const float s2 =
-                __double2float_rn((double)p.tof_sigma2 + (double)__fmaf_rn(l_len, l_len, p.bin2) / 12.0);
-            const float r = __fdiv_rn(__fmul_rn(tt, tt), s2);
-            use = r < 9.0f;
-            val = __fmul_rn(__fmul_rn(R.weight, l_len), p.tof_bin) *
-                  (__expf(-0.5f * r) * rsqrtf(s2) * (1.0f / sqrt2pi));
-        } else {
-            val = __fmul_rn(R.weight, l_len);
-        }
-        n_visits++;
-        if (!f(R.boffs, iz, val, use)) break;
-        last_t = nt;
-        if (i == 0) {
-            R.next_t[0] = __fadd_rn(R.next_t[0], R.delta_t[0]);
-            R.boffs += R.step[0];
-            stillin = --R.in_buf[0];
-        } else if (i == 1) {
-            R.next_t[1] = __fadd_rn(R.next_t[1], R.delta_t[1]);
-            R.boffs += R.step[1];
-            stillin = --R.in_buf[1];
-        } else {
-            R.next_t[2] = __fadd_rn(R.next_t[2], R.delta_t[2]);
-            R.boffs += R.step[2];
-            iz += R.zdir;
-            stillin = --R.in_buf[2];
-        }
-    }
-    return n_visits;
+// Adds four consecutive floats with one reduction (16-byte aligned address). Like a scalar
+// float atomic add, it flushes subnormal inputs and results to zero.
+__device__ __forceinline__ void red_quad(float *q, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};"
+                 :: "l"(q), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
 }
 
-// One thread per ray over the whole image: projection gathers from the image (L2), the
-// scatter ops add with global atomics; kCount counts the visits.
-template <int OP>
+// One thread per ray: RayTracing / BackRayTracing / Map (siddon.cu.cc:293-415) and the
+// visit count. The walk takes the reference's next boundary with its tie order
+// (siddon.cu.cc:305) and advances that axis with selects rather than a branch per axis,
+// so the lanes of a warp (rays crossing boundaries along different axes) stay together.
+//
+// kQuad (scatter ops; the image 16-byte aligned, its voxel count a multiple of 4): a
+// ray's consecutive voxels often share an aligned quad of four floats (runs along x, 1.6
+// voxels per quad on average over the 64x64x32 workload), so the ray gathers its values
+// for the current quad and adds them with one vector reduction when it leaves the quad
+// (the L2 handles reductions at a fixed rate per request, whatever their width: measured
+// 1.47e11 requests/s for 1, 2 or 4 floats). A ray visits each voxel once, so a quad's
+// pending values are set, not summed, and the reduction adds the same value the scalar
+// atomic would. The projection gathers one voxel at a time: its independent loads
+// overlap better than a cached quad load the next voxels wait on (measured: 0.24 against
+// 0.31 ms for 1M rays at 64x64x32; back-projection 0.40 against 0.61 ms with quads).
+template <int OP, bool kQuad>
 __global__ void __launch_bounds__(256) siddon_kernel(const SiddonParams p) {
     const int64_t tid0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    const float sqrt2pi = 2.5066282746310002f;
+    const bool tof = (OP != kMap && OP != kCount) && p.tof_on;
     for (int64_t t = tid0; t < p.n; t += nthreads) {
         Ray R;
         float acc = 0.0f;
         int n_visits = 0;
         if (ray_setup<OP>(p, t, R)) {
-            n_visits = ray_walk<OP>(p, R, [&](int mi, int, float val, bool use) {
-                if (OP == kCount || !use) return true;
-                if (OP == kProj)
-                    acc = fmaf(__ldg(p.image_in + mi), val, acc);
-                else
-                    atomicAdd(p.image_out + mi, val * R.oscale);
-                return true;
-            });
+            int cur = -1;                                  // kQuad: current quad (index / 4)
+            float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);  // its values or pending adds
+            float last_t = 0.0f;
+            int stillin = 1;
+            while (stillin) {
+                // argmin with the reference's tie order (siddon.cu.cc:305)
+                const bool ax = (R.nt0 <= R.nt1) && (R.nt0 <= R.nt2);
+                const bool ay = !(R.nt0 <= R.nt1) && (R.nt1 <= R.nt2);
+                const float nt = ax ? R.nt0 : (ay ? R.nt1 : R.nt2);
+                const float l_len = __fsub_rn(nt, last_t);
+                float val;  // weight * l_len * [TOF] for this voxel
+                bool use = true;
+                if (tof) {
+                    const float tt = __fmaf_rn(-0.5f, __fadd_rn(nt, last_t), R.t_tof);
+                    const float s2 = __double2float_rn(
+                        (double)p.tof_sigma2 + (double)__fmaf_rn(l_len, l_len, p.bin2) / 12.0);
+                    const float r = __fdiv_rn(__fmul_rn(tt, tt), s2);
+                    use = r < 9.0f;
+                    val = __fmul_rn(__fmul_rn(R.weight, l_len), p.tof_bin) *
+                          (__expf(-0.5f * r) * rsqrtf(s2) * (1.0f / sqrt2pi));
+                } else {
+                    val = __fmul_rn(R.weight, l_len);
+                }
+                const int mi = R.boffs;
+                if (OP != kCount && use) {
+                    if (!kQuad) {
+                        if (OP == kProj)
+                            acc = fmaf(__ldg(p.image_in + mi), val, acc);
+                        else
+                            atomicAdd(p.image_out + mi, val * R.oscale);
+                    } else {
+                        const int qd = mi >> 2, r = mi & 3;
+                        if (qd != cur) {
+                            if (cur >= 0) red_quad(p.image_out + 4 * (int64_t)cur, qv.x, qv.y, qv.z, qv.w);
+                            qv = make_float4(0.f, 0.f, 0.f, 0.f);
+                            cur = qd;
+                        }
+                        const float add = val * R.oscale;
+                        qv.x = r == 0 ? add : qv.x;
+                        qv.y = r == 1 ? add : qv.y;
+                        qv.z = r == 2 ? add : qv.z;
+                        qv.w = r == 3 ? add : qv.w;
+                    }
+                }
+                n_visits++;
+                last_t = nt;
+                const bool az = !ax && !ay;
+                R.nt0 = ax ? __fadd_rn(R.nt0, R.dt0) : R.nt0;
+                R.nt1 = ay ? __fadd_rn(R.nt1, R.dt1) : R.nt1;
+                R.nt2 = az ? __fadd_rn(R.nt2, R.dt2) : R.nt2;
+                R.boffs += ax ? R.s0 : (ay ? R.s1 : R.s2);
+                R.in0 -= ax ? 1 : 0;
+                R.in1 -= ay ? 1 : 0;
+                R.in2 -= az ? 1 : 0;
+                stillin = ax ? R.in0 : (ay ? R.in1 : R.in2);
+            }
+            if (kQuad && OP != kProj && OP != kCount && cur >= 0)
+                red_quad(p.image_out + 4 * (int64_t)cur, qv.x, qv.y, qv.z, qv.w);
         }
         if (OP == kProj) p.proj_out[t] = acc;
         if (OP == kCount) p.count_out[t] = n_visits;
     }
 }
 
-// ---------------------------------------------------------------------------------
-// Slab path (projection, back-projection, map, adjoint).
-//
-// The [gz][gy][gx] image is cut into slabs of whole z-slices that fit in shared memory.
-// A binning pass gives every ray the range of slabs its walk can reach (the z indices of
-// its entry voxel and of its exit point, two voxels of margin) and appends it to those
-// slabs' lists. A persistent kernel then gives every CTA an equal share of the slab-major
-// list: per slab it loads the slab (projection) or zeroes it (scatter ops), and each
-// thread replays its ray's exact walk from the entry voxel, touching memory only for the
-// voxels inside the slab and stopping where the walk leaves it (z is monotonic along a
-// ray). Scatter ops add into the slab with shared-memory atomics (3-4x the rate of the
-// L2 atomics the one-thread-per-ray kernel issues) and add the slab to the image once per
-// CTA; the projection adds each ray's per-slab partial sum to its output.
-
-constexpr int kSidThreads = 1024;
-constexpr size_t kSidSlabBytes = 216 * 1024;
-constexpr int kSidMaxSlabs = 32;
-std::atomic<int> g_sid_path{0};  // 0 automatic, 1 slab path, 2 one thread per ray
-
-struct SidPlan {
-    int nz_s, n_slabs;
-    int *count;  // [n_slabs] rays per slab list
-    int *list;   // [n_slabs][n] ray indices
-};
-
-// Slices per slab (balanced over the slabs) and the slab count; false when the slab path
-// does not apply (a slice does not fit, or too many slabs).
-bool sid_geometry(const SiddonParams &p, SidPlan &sp) {
-    const size_t slice = sizeof(float) * (size_t)p.g[0] * p.g[1];
-    const int max_nz = (int)std::min<size_t>((size_t)p.g[2], kSidSlabBytes / slice);
-    if (max_nz < 1) return false;
-    sp.n_slabs = (p.g[2] + max_nz - 1) / max_nz;
-    if (sp.n_slabs > kSidMaxSlabs) return false;
-    sp.nz_s = (p.g[2] + sp.n_slabs - 1) / sp.n_slabs;
-    sp.n_slabs = (p.g[2] + sp.nz_s - 1) / sp.nz_s;
-    return p.n < (int64_t)INT32_MAX;
-}
-
-template <int OP>
-__global__ void __launch_bounds__(256) sid_bin_kernel(const SiddonParams p, SidPlan sp) {
-    const int64_t tid0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    // whole warps iterate together (the list appends are warp-aggregated)
-    for (int64_t base = tid0 - lane; base < p.n; base += nthreads) {
-        const int64_t t = base + lane;
-        int k_lo = 0, k_hi = -1;
-        Ray R;
-        if (t < p.n && ray_setup<OP>(p, t, R)) {
-            // The walk runs to the grid's edge, not to the ray's end point (it stops only
-            // when a voxel counter runs out, siddon.cu.cc:302), so its last z is where
-            // the first axis leaves the grid: t_end (from the entry point) = min over the
-            // moving axes of next_t + (in_buf - 1) delta_t; z in the box-corner frame.
-            float t_end = INFINITY;
-#pragma unroll
-            for (int a = 0; a < 3; a++)
-                if (R.step[a] != 0)
-                    t_end = fminf(t_end, fmaf((float)(R.in_buf[a] - 1), R.delta_t[a], R.next_t[a]));
-            const float zt = fmaf(R.tmin + t_end, R.dirz, R.z0);
-            const float fz = fminf(fmaxf(floorf(zt / p.v_res[2]), -4.0f), (float)p.g[2] + 4.0f);
-            const int izt = (int)fz;
-            const int lo = max(0, min(R.pos[2], izt) - 2);
-            const int hi = min(p.g[2] - 1, max(R.pos[2], izt) + 2);
-            k_lo = lo / sp.nz_s;
-            k_hi = hi / sp.nz_s;
-        }
-        for (int k = 0; k < sp.n_slabs; k++) {
-            const bool in = k >= k_lo && k <= k_hi;
-            const unsigned m = __ballot_sync(0xffffffffu, in);
-            if (!m) continue;
-            int first = 0;
-            if (lane == __ffs(m) - 1) first = atomicAdd(sp.count + k, __popc(m));
-            first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
-            if (in) sp.list[(int64_t)k * p.n + first + __popc(m & ((1u << lane) - 1u))] = (int)t;
-        }
-    }
-}
-
-template <int OP>
-__global__ void __launch_bounds__(kSidThreads, 1) siddon_slab_kernel(const SiddonParams p,
-                                                                    SidPlan sp) {
-    extern __shared__ float slab[];
-    __shared__ int64_t offs[kSidMaxSlabs + 1];
-    if (threadIdx.x == 0) {
-        int64_t acc = 0;
-        for (int k = 0; k < sp.n_slabs; k++) {
-            offs[k] = acc;
-            acc += sp.count[k];
-        }
-        offs[sp.n_slabs] = acc;
-    }
-    __syncthreads();
-    const int64_t total = offs[sp.n_slabs];
-    const int64_t g = blockIdx.x, G = gridDim.x;
-    const int64_t lo = total * g / G, hi = total * (g + 1) / G;
-    const int slice = p.g[0] * p.g[1];
-    int k = 0;
-    for (int64_t pos = lo; pos < hi;) {
-        while (offs[k + 1] <= pos) k++;
-        const int64_t end = min(hi, offs[k + 1]);
-        const int Z0 = k * sp.nz_s, Z1 = min(Z0 + sp.nz_s, p.g[2]);
-        const int nvox = (Z1 - Z0) * slice;
-        const int64_t base = (int64_t)Z0 * slice;
-        if (OP == kProj) {
-            for (int i = threadIdx.x; i < nvox; i += kSidThreads) slab[i] = __ldg(p.image_in + base + i);
-        } else {
-            for (int i = threadIdx.x; i < nvox; i += kSidThreads) slab[i] = 0.0f;
-        }
-        __syncthreads();
-        for (int64_t q = pos + threadIdx.x; q < end; q += kSidThreads) {
-            const int t = sp.list[(int64_t)k * p.n + (q - offs[k])];
-            Ray R;
-            if (!ray_setup<OP>(p, t, R)) continue;
-            float acc = 0.0f;
-            ray_walk<OP>(p, R, [&](int mi, int iz, float val, bool use) {
-                if (iz < Z0 || iz >= Z1) {
-                    // not in the slab: keep walking only towards it (z is monotonic)
-                    return (R.zdir > 0 && iz < Z0) || (R.zdir < 0 && iz >= Z1);
-                }
-                // a visited voxel is in the grid, so iz in [Z0, Z1) puts mi - base in
-                // [0, (Z1 - Z0) gx gy)
-                if (!use) return true;
-                if (OP == kProj)
-                    acc = fmaf(slab[mi - base], val, acc);
-                else
-                    atomicAdd(&slab[mi - base], val * R.oscale);
-                return true;
-            });
-            if (OP == kProj && acc != 0.0f) atomicAdd(p.proj_out + t, acc);
-        }
-        __syncthreads();
-        if (OP != kProj) {
-            for (int i = threadIdx.x; i < nvox; i += kSidThreads) {
-                const float v = slab[i];
-                if (v != 0.0f) atomicAdd(p.image_out + base + i, v);
-            }
-            __syncthreads();
-        }
-        pos = end;
-    }
-}
+// Kernel family (srf_siddon_set_tuning): 0 automatic (quads for the scatter ops where the
+// image allows), 1 one load / atomic per voxel.
+std::atomic<int> g_sid_path{0};
 
 int siddon_setup(SiddonParams &p, const int *grid, const float *center, const float *size,
                  float tof_bin, float tof_sigma2, int64_t n, int64_t lor_stride) {
@@ -407,62 +293,19 @@ int siddon_setup(SiddonParams &p, const int *grid, const float *center, const fl
     return SRF_OK;
 }
 
-// The slab path for p's op: bins the rays, then one persistent launch. Returns -1 when
-// it does not apply.
-template <int OP>
-int siddon_launch_slab(const SiddonParams &p, cudaStream_t stream) {
-    SidPlan sp{};
-    if (!sid_geometry(p, sp)) return -1;
-    const size_t b_count = 256;
-    const size_t b_list = sizeof(int) * (size_t)sp.n_slabs * (size_t)p.n;
-    char *ws = nullptr;
-    cudaError_t e = scratch_alloc((void **)&ws, b_count + b_list, stream);
-    if (e != cudaSuccess) {
-        set_cuda_error(e);
-        return SRF_ERR_CUDA;
-    }
-    sp.count = reinterpret_cast<int *>(ws);
-    sp.list = reinterpret_cast<int *>(ws + b_count);
-    static std::atomic<unsigned long long> attr_set{0};  // per device
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
-    e = cudaSuccess;
-    if (!(attr_set.load() & (1ull << dev))) {
-        e = cudaFuncSetAttribute(siddon_slab_kernel<OP>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSidSlabBytes);
-        if (e == cudaSuccess) attr_set.fetch_or(1ull << dev);
-    }
-    if (e == cudaSuccess) e = cudaMemsetAsync(sp.count, 0, b_count, stream);
-    if (e == cudaSuccess && OP == kProj)
-        e = cudaMemsetAsync(p.proj_out, 0, sizeof(float) * (size_t)p.n, stream);
-    if (e != cudaSuccess) {
-        set_cuda_error(e);
-        cudaFreeAsync(ws, stream);
-        return SRF_ERR_CUDA;
-    }
-    sid_bin_kernel<OP><<<stride_grid(p.n, 256, 8), 256, 0, stream>>>(p, sp);
-    const size_t smem = sizeof(float) * (size_t)sp.nz_s * p.g[0] * p.g[1];
-    siddon_slab_kernel<OP><<<num_sms(), kSidThreads, smem, stream>>>(p, sp);
-    count_launches(2);
-    int st = check_launch();
-    e = cudaFreeAsync(ws, stream);
-    if (st == SRF_OK && e != cudaSuccess) {
-        set_cuda_error(e);
-        st = SRF_ERR_CUDA;
-    }
-    return st;
-}
-
 template <int OP>
 int siddon_launch(const SiddonParams &p, cudaStream_t stream) {
     if (p.n == 0) return SRF_OK;
-    if (OP != kCount && g_sid_path.load(std::memory_order_relaxed) != 2) {
-        const int st = siddon_launch_slab<OP>(p, stream);
-        if (st >= 0) return st;
-    }
     const int block = 256;
     const int grid = stride_grid(p.n, block, 8);
-    siddon_kernel<OP><<<grid, block, 0, stream>>>(p);
+    constexpr bool kScatter = OP == kBack || OP == kMap || OP == kAdj;
+    const bool quad = kScatter && g_sid_path.load(std::memory_order_relaxed) == 0 &&
+                      (reinterpret_cast<uintptr_t>(p.image_out) & 15u) == 0 &&
+                      ((int64_t)p.g[0] * p.g[1] * p.g[2]) % 4 == 0;
+    if (quad)
+        siddon_kernel<OP, kScatter><<<grid, block, 0, stream>>>(p);
+    else
+        siddon_kernel<OP, false><<<grid, block, 0, stream>>>(p);
     count_launches(1);
     return check_launch();
 }
@@ -578,11 +421,10 @@ extern "C" int srf_siddon_count_samples(const float *x1, const float *y1, const 
     return siddon_launch<kCount>(p, (cudaStream_t)stream);
 }
 
-// No counterpart in the reference: the Siddon kernel family (0 automatic: the
-// shared-memory slab path where a z-slice fits and the image has at most 32 slabs,
-// 1 the same, 2 one thread per ray with L2 gathers and atomics).
+// No counterpart in the reference: the Siddon kernel family (0 automatic: the scatter ops
+// reduce four consecutive voxels at a time where the image allows; 1 one per voxel).
 extern "C" int srf_siddon_set_tuning(int path) {
-    if (path < 0 || path > 2) return SRF_ERR_INVALID_ARGUMENT;
+    if (path < 0 || path > 1) return SRF_ERR_INVALID_ARGUMENT;
     g_sid_path.store(path);
     return SRF_OK;
 }

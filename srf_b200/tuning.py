@@ -29,6 +29,13 @@ def set_tuning(path=0, slab_slices=0, grid_mult=0):
     return (path, slab_slices, grid_mult)
 
 
+def set_siddon_tuning(path=0):
+    """Siddon kernel family (``srf_siddon_set_tuning``): 0 automatic (the scatter ops
+    reduce four consecutive voxels at a time where the image allows), 1 one per voxel."""
+    _lib.call("srf_siddon_set_tuning", int(path))
+    return path
+
+
 def set_scratch_limit(nbytes=0):
     """Bound the per-call scratch of the slab kernels (``srf_tor_set_scratch_limit``);
     larger calls run in chunks of LORs. 0 restores the default (1 GiB)."""

@@ -198,13 +198,22 @@ def scase():
 SID_PARAMS = {"tof530": 530.0, "tofdefault": 1.0e4, "notof": None}
 
 
+@pytest.fixture(params=[0, 1], ids=["quad", "scalar"])
+def sid_path(request):
+    """The Siddon kernel family: scatter ops reduce quads of voxels, or one per voxel."""
+    from srf_b200 import tuning
+    tuning.set_siddon_tuning(request.param)
+    yield request.param
+    tuning.set_siddon_tuning(0)
+
+
 def _sp(name):
     b, s2 = K.tof_params(530.0 if SID_PARAMS[name] is None else SID_PARAMS[name])
     return b, (1.0e6 if SID_PARAMS[name] is None else s2)
 
 
 @pytest.mark.parametrize("pname", list(SID_PARAMS))
-def test_siddon_projection_backprojection(scase, pname):
+def test_siddon_projection_backprojection(scase, pname, sid_path):
     b, s2 = _sp(pname)
     args = (scase["grid"], scase["center"], scase["size"])
     lors, img = scase["lors"], scase["kimage"]
@@ -225,7 +234,7 @@ def test_siddon_projection_backprojection(scase, pname):
     assert e32 <= TOL and e64 <= FP64_TOL["siddon_image"], (e32, e64)
 
 
-def test_siddon_maplors_and_adjoint(scase):
+def test_siddon_maplors_and_adjoint(scase, sid_path):
     args = (scase["grid"], scase["center"], scase["size"])
     lors = scase["lors"]
     vals = (0.5 + np.random.default_rng(5).random(lors.shape[1])).astype(np.float32)
