@@ -112,6 +112,28 @@ int srf_tor_backproject_adjoint(const float *x1, const float *y1, const float *z
                                 float tof_sigma2, float *image, int64_t num_events,
                                 int64_t lor_stride, int accumulate, void *stream);
 
+/* No counterpart in the reference as one call: the effmap's Maplors (tor.cu.cc:435-481)
+ * of detector-pair LORs that never exist in memory. LORs number first .. first+count-1 of
+ * a generated sequence are taken through map_process (on_tor_lors.py:243-248) and those
+ * of dominant-axis group `axis` (0 x, 1 y, 2 z) are mapped with lors_value = 1 into
+ * `image`, in that group's kernel layout (grid / center / size as for srf_tor_maplors).
+ * Every kernel of the call makes LOR t again from its number:
+ *   kind 0: a uniform pair of distinct crystals: a = floor(u1 n / 2^32),
+ *           b = floor(u2 (n - 1) / 2^32) shifted up past a, (u1, u2) the high and low
+ *           halves of SplitMix64 output first + t of the stream seeded `seed`, n the
+ *           crystal count;
+ *   kind 1: the scanner's block-pair enumeration in the reference's order (ring pairs
+ *           ir1-major, srfapp_new.py:153-157; block pairs i1 < i2 in a ring, i1 != i2
+ *           across rings, scanner/pet/pet.py:149-168; every crystal of the first block,
+ *           major, with every crystal of the second, :170-177).
+ * crystals: DEVICE float32 [n_rings * n_blocks * n_per_block][3] crystal centres, ring
+ * major, then block, then crystal in the block's mesh order. */
+int srf_tor_maplors_generated(int kind, const float *crystals, int n_rings, int n_blocks,
+                              int n_per_block, unsigned long long seed, int64_t first,
+                              int64_t count, int axis, int geo_sigma2_flag, const int *grid,
+                              const float *center, const float *size, float kernel_width,
+                              float *image, int accumulate, void *stream);
+
 /* No counterpart in the reference: per-LOR work counts of the TOR operator, used for
  * the roofline (algorithmic samples) and for work estimation. counts[i] = patch voxels
  * with non-zero weight (inside the 3-sigma tube), counts[num_events + i] = window
@@ -314,6 +336,17 @@ int srf_mlem_update(float *image, const float *effinv, const float *bp, int64_t 
  * All DEVICE pointers. The adjoint is the same call with the CSR of A^T. */
 int srf_csr_spmm(const int64_t *rowptr, const int *col, const float *val, int64_t nrows,
                  int64_t ncols, const float *x, int nz, float *y, int accumulate, void *stream);
+
+/* Separable PSF of the PSF reconstruction step in one launch (PSFReconStep,
+ * src/python/srf/model/recon_step.py:78-87 and :95-101, there a dense matmul followed by
+ * tf.sparse_tensor_dense_matmul): y = A (x Pz^T) (transpose_pz = 0, the forward PSF) or
+ * y = A (x Pz) (transpose_pz = 1; with the CSR of A^T this is the adjoint), A an
+ * [nrows, ncols] CSR matrix as in srf_csr_spmm, x [ncols, nz], Pz a dense row-major
+ * [nz, nz] matrix, y [nrows, nz] (y += ... with accumulate != 0). nz <= 224
+ * (SRF_ERR_UNSUPPORTED above). All DEVICE pointers. */
+int srf_psf_apply(const int64_t *rowptr, const int *col, const float *val, int64_t nrows,
+                  int64_t ncols, const float *x, int nz, const float *pz, int transpose_pz,
+                  float *y, int accumulate, void *stream);
 
 /* ------------------------------------------------------------------------ peak probes */
 

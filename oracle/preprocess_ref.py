@@ -166,3 +166,21 @@ def merge_effmap(total, keep, threshold=1e-6, zero_below=True):
     if zero_below:
         out[~hi] = 0
     return out
+
+
+def psf_forward(psf_xy, psf_z, image):
+    """``PSFReconStep.kernel`` forward PSF (src/python/srf/model/recon_step.py:78-87): the
+    image as an [nx*ny, nz] matrix, times psf_z^T (dense), then the sparse transaxial
+    matrix from the left (tf.sparse_tensor_dense_matmul), reshaped back. ``psf_xy``: a
+    scipy sparse or dense [nx*ny, nx*ny] matrix; arithmetic in the inputs' precision."""
+    nx, ny, nz = image.shape
+    v = image.reshape(nx * ny, nz) @ psf_z.T
+    return np.asarray(psf_xy @ v).reshape(nx, ny, nz)
+
+
+def psf_adjoint(psf_xy, psf_z, image):
+    """The back-projection side of the same step (recon_step.py:95-101): the image as an
+    [nx*ny, nz] matrix times psf_z, then the transposed sparse matrix from the left."""
+    nx, ny, nz = image.shape
+    v = image.reshape(nx * ny, nz) @ psf_z
+    return np.asarray(psf_xy.T @ v).reshape(nx, ny, nz)

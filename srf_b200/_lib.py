@@ -53,6 +53,8 @@ SIGNATURES = {
     "srf_tor_set_tuning": ([_int, _int, _int], _int),
     "srf_siddon_set_tuning": ([_int], _int),
     "srf_tor_set_scratch_limit": ([_i64], _int),
+    "srf_tor_maplors_generated": ([_int, _p, _int, _int, _int, C.c_uint64, _i64, _i64, _int,
+                                   _int, _p, _p, _p, _f, _p, _int, _p], _int),
     "srf_tor_count_samples": ([_p] * 7 + [_int, _p, _p, _p, _f, _p, _i64, _i64, _p], _int),
     "srf_siddon_count_samples": ([_p] * 6 + [_p, _p, _p, _p, _i64, _i64, _p], _int),
     "srf_mlem_update": ([_p, _p, _p, _i64, _p], _int),
@@ -61,6 +63,7 @@ SIGNATURES = {
     "srf_map_process": ([_p, _i64, _i64, _p, _p, _p, _i64, _p], _int),
     "srf_recon_process_noalloc": ([_p, _i64, _i64, C.c_double, _p, _p, _p], _int),
     "srf_csr_spmm": ([_p, _p, _p, _i64, _i64, _p, _int, _p, _int, _p], _int),
+    "srf_psf_apply": ([_p, _p, _p, _i64, _i64, _p, _int, _p, _int, _p, _int, _p], _int),
     "srf_order_by_direction": ([_p, _i64, _int, _i64, _p, _p], _int),
     "srf_probe_threads": ([_p], _int),
     "srf_probe_l2_read": ([_p, _i64, _int, _p, _p], _int),

@@ -26,6 +26,7 @@
 #include <cstdlib>
 #include <type_traits>
 
+#include "lor_prep.cuh"
 #include "srf_common.cuh"
 
 namespace srf {
@@ -69,7 +70,128 @@ struct TorParams {
     const int *frame;
     int64_t frame_stride;
     int n_frames;
+    // Map LORs made on the fly (srf_tor_maplors_generated): gen = 0 LOR columns in memory;
+    // 1 uniform random crystal pairs; 2 every crystal pair of the scanner's block pairs.
+    // LOR t of the call is number gen_first + t of that sequence, taken through
+    // map_process and kept when its dominant axis is gen_axis; its value is 1.
+    int gen, gen_axis;
+    int64_t gen_first;
+    unsigned long long gen_seed;
+    const float *crystals;  // [n_rings * n_blocks * n_per_block][3] crystal centres
+    int n_rings, n_blocks, n_per_block;
 };
+
+// ---------------------------------------------------------------------------------
+// Generated detector-pair LORs (map calls). The random pairs use SplitMix64 (Steele, Lea
+// and Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014): output k of
+// the stream seeded s is the finaliser applied to s + (k + 1) * 0x9E3779B97F4A7C15.
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long s,
+                                                         unsigned long long k) {
+    unsigned long long z = s + (k + 1ull) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Crystal indices (a, b) of LOR number g.
+//   gen 1: a = floor(u1 n / 2^32), b = floor(u2 (n - 1) / 2^32) shifted up past a, with
+//          (u1, u2) the high and low halves of splitmix64(seed, g) and n the crystal count;
+//   gen 2: the g-th pair of the reference's effmap enumeration (srfapp_new.py:153-157 over
+//          scanner/pet/pet.py:149-177): ring pairs (ir1, ir2) ir1-major, in each the block
+//          pairs i1 < i2 (same ring) or i1 != i2 (different rings) row-major, in each every
+//          crystal of the first block (major) with every crystal of the second.
+__device__ __forceinline__ void gen_pair(const TorParams &p, long long g, int &a, int &b) {
+    if (p.gen == 1) {
+        const unsigned n = (unsigned)(p.n_rings * p.n_blocks * p.n_per_block);
+        const unsigned long long h = splitmix64(p.gen_seed, (unsigned long long)g);
+        const unsigned u1 = (unsigned)(h >> 32), u2 = (unsigned)h;
+        a = (int)(((unsigned long long)u1 * n) >> 32);
+        const int j = (int)(((unsigned long long)u2 * (n - 1u)) >> 32);
+        b = j + (j >= a ? 1 : 0);
+        return;
+    }
+    const long long nb = p.n_blocks, cb = (long long)p.n_per_block * p.n_per_block;
+    const long long n_same = nb * (nb - 1) / 2 * cb, n_cross = nb * (nb - 1) * cb;
+    const long long row = (long long)(p.n_rings - 1) * n_cross + n_same;  // one ir1
+    const long long ir1 = g / row;
+    long long r = g - ir1 * row;
+    long long ir2;
+    if (r < ir1 * n_cross) {
+        ir2 = r / n_cross;
+        r -= ir2 * n_cross;
+    } else if (r < ir1 * n_cross + n_same) {
+        ir2 = ir1;
+        r -= ir1 * n_cross;
+    } else {
+        const long long q = r - ir1 * n_cross - n_same;
+        ir2 = ir1 + 1 + q / n_cross;
+        r = q - (ir2 - ir1 - 1) * n_cross;
+    }
+    const long long bp = r / cb, rc = r - bp * cb;
+    long long i1, i2;
+    if (ir1 == ir2) {
+        // row i of the strict upper triangle holds nb - 1 - i pairs and starts at
+        // i (2 nb - i - 1) / 2; estimate i from the quadratic, then correct exactly
+        const double bb = 2.0 * (double)nb - 1.0;
+        long long i = (long long)floor((bb - sqrt(fmax(bb * bb - 8.0 * (double)bp, 0.0))) / 2.0);
+        i = max(0ll, min(i, nb - 2));
+        while (i > 0 && i * (2 * nb - i - 1) / 2 > bp) i--;
+        while (i < nb - 2 && (i + 1) * (2 * nb - i - 2) / 2 <= bp) i++;
+        i1 = i;
+        i2 = i + 1 + (bp - i * (2 * nb - i - 1) / 2);
+    } else {
+        i1 = bp / (nb - 1);
+        const long long j = bp - i1 * (nb - 1);
+        i2 = j + (j >= i1 ? 1 : 0);
+    }
+    const long long c1 = rc / p.n_per_block, c2 = rc - c1 * p.n_per_block;
+    a = (int)((ir1 * nb + i1) * p.n_per_block + c1);
+    b = (int)((ir2 * nb + i2) * p.n_per_block + c2);
+}
+
+// The map record columns of generated LOR t (x1, y1, z1, x2, y2, z2, f after
+// map_process's swap and permutation); false when its dominant axis is another group's.
+__device__ __forceinline__ bool gen_columns(const TorParams &p, int64_t t, float (&c)[7]) {
+    int a, b;
+    gen_pair(p, (long long)(p.gen_first + t), a, b);
+    float e[6];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        e[k] = __ldg(p.crystals + 3 * (int64_t)a + k);
+        e[3 + k] = __ldg(p.crystals + 3 * (int64_t)b + k);
+    }
+    const Rec r = process<false>(e, false, 0.0f);  // map_process (on_tor_lors.py:243-248)
+    if (r.bucket >= kBuckets || (r.bucket >> 1) != p.gen_axis) return false;
+#pragma unroll
+    for (int k = 0; k < 7; k++) c[k] = r.v[k];
+    return true;
+}
+
+// LOR t's endpoints and sigma^2 factor (from memory, or generated); false for a generated
+// LOR of another axis group.
+// kGen: the call's LORs are generated (TorParams::gen), map calls only.
+template <int OP, bool kGen>
+__device__ __forceinline__ bool lor_columns(const TorParams &p, int64_t t, float &x1, float &y1,
+                                            float &z1, float &x2, float &y2, float &z2,
+                                            float &f) {
+    if constexpr (kGen) {
+        static_assert(OP == kMap, "generated LORs are map LORs");
+        float c[7];
+        if (!gen_columns(p, t, c)) return false;
+        x1 = c[0]; y1 = c[1]; z1 = c[2]; x2 = c[3]; y2 = c[4]; z2 = c[5]; f = c[6];
+        return true;
+    }
+    const int64_t o = t * p.stride;
+    x1 = __ldg(p.x1 + o); y1 = __ldg(p.y1 + o); z1 = __ldg(p.z1 + o);
+    x2 = __ldg(p.x2 + o); y2 = __ldg(p.y2 + o); z2 = __ldg(p.z2 + o);
+    f = __ldg(p.f + o);
+    return true;
+}
+
+// The map's divisor of LOR t (the caller's lors_value; 1 for generated LORs).
+__device__ __forceinline__ float map_value(const TorParams &p, int64_t t) {
+    return p.values ? __ldg(p.values + t) : 1.0f;
+}
 
 __device__ __forceinline__ int64_t frame_offset(const TorParams &p, int64_t t) {
     return p.frame ? (int64_t)__ldg(p.frame + t) * p.frame_stride : 0;
@@ -111,9 +233,17 @@ __device__ __noinline__ void generic_lor(const TorParams &p, int64_t t, int lane
     const int64_t slice_mesh = (int64_t)p.gx * p.gy;
     const int64_t img0 = frame_offset(p, t);
     const int64_t o = t * p.stride;
-    const float x1 = __ldg(p.x1 + o), y1 = __ldg(p.y1 + o), z1 = __ldg(p.z1 + o);
-    const float x2 = __ldg(p.x2 + o), y2 = __ldg(p.y2 + o), z2 = __ldg(p.z2 + o);
-    const float f = __ldg(p.f + o);
+    float x1, y1, z1, x2, y2, z2, f;
+    bool have;
+    if constexpr (OP == kMap)
+        have = p.gen ? lor_columns<OP, true>(p, t, x1, y1, z1, x2, y2, z2, f)
+                     : lor_columns<OP, false>(p, t, x1, y1, z1, x2, y2, z2, f);
+    else
+        have = lor_columns<OP, false>(p, t, x1, y1, z1, x2, y2, z2, f);
+    if (!have) {
+        if (OP == kCount && lane == 0) p.count_out[t] = p.count_out[p.n + t] = 0;
+        return;
+    }
 
     // Per-LOR output scale and the early-outs of the reference's value tests.
     float scale = p.tof_scale;
@@ -123,7 +253,7 @@ __device__ __noinline__ void generic_lor(const TorParams &p, int64_t t, int lane
         if (!((double)v > 1e-7)) return;  // tor.cu.cc:203
         scale = __fdiv_rn(p.tof_scale, v);
     } else if (OP == kMap) {
-        float v = __ldg(p.values + t);
+        float v = map_value(p, t);
         scale = __fdiv_rn(1.0f, v);  // tor.cu.cc:239 divides without a threshold
         all_slots = !(fabsf(scale) <= 3.0e38f);
     } else if (OP == kAdj) {
@@ -262,7 +392,7 @@ struct LorConst {
 // The per-LOR constants that do not depend on the op's values: direction, cut-off and
 // exponent slope, bounding-box half-extents, TOF centre and candidate slices. Returns
 // false when no crossing is possible (degenerate or non-finite LOR, bad frame id).
-template <int OP>
+template <int OP, bool kGen = false>
 __device__ __forceinline__ bool lor_geometry(const TorParams &p, int64_t t, LorConst &L) {
     L.all = false;
     L.scale = p.tof_scale;
@@ -271,9 +401,8 @@ __device__ __forceinline__ bool lor_geometry(const TorParams &p, int64_t t, LorC
     L.s_hi = -1;
     if (!frame_ok(p, t)) return false;
     const int64_t o = t * p.stride;
-    const float x1 = __ldg(p.x1 + o), y1 = __ldg(p.y1 + o), z1 = __ldg(p.z1 + o);
-    const float x2 = __ldg(p.x2 + o), y2 = __ldg(p.y2 + o), z2 = __ldg(p.z2 + o);
-    const float f = __ldg(p.f + o);
+    float x1, y1, z1, x2, y2, z2, f;
+    if (!lor_columns<OP, kGen>(p, t, x1, y1, z1, x2, y2, z2, f)) return false;
     L.x1 = x1;
     L.y1 = y1;
     L.z1 = z1;
@@ -333,7 +462,7 @@ __device__ __forceinline__ bool lor_value_scale(const TorParams &p, int64_t t, L
         const float m = frexpf(L.scale, &e);
         L.k0s = (float)e + __log2f(m);
     } else if (OP == kMap) {
-        L.scale = __fdiv_rn(1.0f, __ldg(p.values + t));  // tor.cu.cc:239, no threshold
+        L.scale = __fdiv_rn(1.0f, map_value(p, t));  // tor.cu.cc:239, no threshold
         L.all = !(fabsf(L.scale) <= 3.0e38f);  // w/0 or w/NaN lands on every visited voxel
         if (L.all) L.bxv = L.byv = 1.0e9f;     // ... so the whole window is walked
     } else if (OP == kAdj) {
@@ -344,10 +473,27 @@ __device__ __forceinline__ bool lor_value_scale(const TorParams &p, int64_t t, L
 
 // Loads LOR t and derives its constants. Returns false when the LOR contributes
 // nothing (no crossing possible, or a back-projection value at/below 1e-7).
-template <int OP>
+template <int OP, bool kGen = false>
 __device__ __forceinline__ bool lor_prepare(const TorParams &p, int64_t t, LorConst &L) {
-    if (!lor_geometry<OP>(p, t, L)) return false;
+    if (!lor_geometry<OP, kGen>(p, t, L)) return false;
     return lor_value_scale<OP>(p, t, L);
+}
+
+// lor_geometry / lor_prepare for a call whose LORs may be generated (map calls).
+template <int OP>
+__device__ __forceinline__ bool geometry_any(const TorParams &p, int64_t t, LorConst &L) {
+    if constexpr (OP == kMap) {
+        if (p.gen) return lor_geometry<OP, true>(p, t, L);
+    }
+    return lor_geometry<OP, false>(p, t, L);
+}
+
+template <int OP>
+__device__ __forceinline__ bool prepare_any(const TorParams &p, int64_t t, LorConst &L) {
+    if constexpr (OP == kMap) {
+        if (p.gen) return lor_prepare<OP, true>(p, t, L);
+    }
+    return lor_prepare<OP, false>(p, t, L);
 }
 
 // The binning pass stores each LOR's geometry once as a 64-byte record, so the slab
@@ -598,7 +744,7 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
     const int64_t slice_mesh = (int64_t)p.gx * p.gy;
     for (int64_t t = warp; t < p.n; t += nwarps) {
         LorConst L;
-        const bool any = lor_prepare<OP>(p, t, L);
+        const bool any = prepare_any<OP>(p, t, L);
         float acc = 0.0f;
         int n_useful = 0, n_slots = 0;
         if (any) {
@@ -675,6 +821,22 @@ struct SegPlan {
     LorRec *rec;           // [n] per-LOR records written by seg_count
 };
 
+// LOR t's constants in a slab kernel: from the record the binning wrote, or, for generated
+// map LORs (no records: nothing per LOR is kept in memory), derived again from the LOR.
+template <int OP, bool kGen>
+__device__ __forceinline__ bool slab_lor(const TorParams &p, const SegPlan &sp, int64_t t,
+                                         LorConst &L) {
+    if constexpr (kGen) return lor_prepare<OP, true>(p, t, L);
+    return lor_load<OP>(p, sp.rec, t, L);
+}
+
+template <int OP, bool kGen>
+__device__ __forceinline__ bool slab_lor_geometry(const TorParams &p, const SegPlan &sp,
+                                                  int64_t t, LorConst &L) {
+    if constexpr (kGen) return lor_geometry<OP, true>(p, t, L);
+    return lor_rec_geometry(sp.rec, t, L);
+}
+
 // Slab ids of LOR t (slice range k of its frame, row band b): id = k * nbands + b, with k
 // counted over frames. Calls g(id) for each. With row bands, the bands of slice range k
 // are those the LOR's window rows can reach in its slices there: the rows follow the
@@ -738,13 +900,15 @@ __global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams 
         if (t >= p.n) break;
         int packed = -1;
         LorConst L;
-        bool ok = lor_geometry<OP>(p, t, L);
-        const LorRec r = make_rec(L, ok);
-        float4 *q = reinterpret_cast<float4 *>(sp.rec + t);
-        q[0] = r.a;
-        q[1] = r.b;
-        q[2] = r.c;
-        q[3] = r.d;
+        bool ok = geometry_any<OP>(p, t, L);
+        if (sp.rec) {
+            const LorRec r = make_rec(L, ok);
+            float4 *q = reinterpret_cast<float4 *>(sp.rec + t);
+            q[0] = r.a;
+            q[1] = r.b;
+            q[2] = r.c;
+            q[3] = r.d;
+        }
         if (ok && OP == kBack) ok = (double)__ldg(p.values + t) > 1e-7;  // tor.cu.cc:203
         if (ok) {
             const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
@@ -822,7 +986,7 @@ __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p
         const int k_lo = packed & 0xffff, k_hi = packed >> 16;
         int s_lo = 0, s_hi = p.gz - 1;
         float y1 = 0.f, z1 = 0.f, d1 = 0.f, dz = 1.f;
-        if (kBand) {  // the values seg_count used, from the LOR's record
+        if (kBand && sp.rec) {  // the values seg_count used, from the LOR's record
             const float4 *q = reinterpret_cast<const float4 *>(sp.rec + t);
             const float4 a = q[0], b = q[1], d = q[3];
             const int sl = __float_as_int(d.w);
@@ -832,6 +996,15 @@ __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p
             z1 = a.z;
             d1 = b.x;
             dz = b.y;
+        } else if (kBand) {  // generated map LORs: the same values, derived again
+            LorConst L;
+            lor_geometry<kMap, true>(p, t, L);
+            s_lo = L.s_lo;
+            s_hi = L.s_hi;
+            y1 = L.y1;
+            z1 = L.z1;
+            d1 = L.d1;
+            dz = L.dz;
         }
         lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi, y1, z1, d1, dz, [&](int id) {
             const int pos = warp_increment(cursor, id);
@@ -868,7 +1041,7 @@ __host__ __device__ __forceinline__ int slab_floats(int nsl, int gx, int gy, int
 // at a time (one item per lane, the LOR's constants read from its record); otherwise
 // each lane walks its own segment's slices.
 // kBand: the slabs are bands of rows (sp.nbands > 1), so rows are limited to the band.
-template <int OP, int P, bool kExpand, bool kBand>
+template <int OP, int P, bool kExpand, bool kBand, bool kGen = false>
 __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorParams p, SegPlan sp) {
     extern __shared__ float slab[];
     __shared__ signed char owner_tab[kSlabThreads / 32][32];
@@ -929,7 +1102,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
             int a = 0, cnt = 0, t = -1;
             if (q < end) {
                 t = sp.seg[q];
-                if (lor_load<OP>(p, sp.rec, t, L)) {
+                if (slab_lor<OP, kGen>(p, sp, t, L)) {
                     a = max(L.s_lo, S0);
                     cnt = max(0, min(L.s_hi, S1 - 1) - a + 1);
                 }
@@ -982,7 +1155,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                 const float k0s_o = __shfl_sync(0xffffffffu, L.k0s, o);
                 const bool all_o = OP == kMap && __shfl_sync(0xffffffffu, (int)L.all, o);
                 if (valid) {
-                    lor_rec_geometry(sp.rec, t_o, M);
+                    slab_lor_geometry<OP, kGen>(p, sp, t_o, M);
                     M.scale = scale_o;
                     M.k0s = k0s_o;
                     M.all = all_o;
@@ -1171,6 +1344,7 @@ TorParams lor_chunk(const TorParams &p, int64_t c0, int64_t n) {
     if (q.values) q.values += c0;
     if (q.proj_out) q.proj_out += c0;
     if (q.frame) q.frame += c0;
+    q.gen_first += c0;
     q.n = n;
     return q;
 }
@@ -1182,8 +1356,17 @@ int slab_kernel(const TorParams &p, bool band, void (**kern)(const TorParams, Se
     *kern = p.slab_expand
                 ? (band ? tor_slab_kernel<OP, P, true, true> : tor_slab_kernel<OP, P, true, false>)
                 : (band ? tor_slab_kernel<OP, P, false, true> : tor_slab_kernel<OP, P, false, false>);
-    static std::atomic<unsigned long long> attr_set[4];  // per kernel instance, per device
-    std::atomic<unsigned long long> &done = attr_set[(p.slab_expand ? 2 : 0) + (band ? 1 : 0)];
+    int which = (p.slab_expand ? 2 : 0) + (band ? 1 : 0);
+    if constexpr (OP == kMap) {
+        // generated LORs: their own instances, so the others carry no generator code
+        if (p.gen) {
+            *kern = band ? tor_slab_kernel<OP, P, false, true, true>
+                         : tor_slab_kernel<OP, P, false, false, true>;
+            which = 4 + (band ? 1 : 0);
+        }
+    }
+    static std::atomic<unsigned long long> attr_set[6];  // per kernel instance, per device
+    std::atomic<unsigned long long> &done = attr_set[which];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
     if (!(done.load() & (1ull << dev))) {
@@ -1212,7 +1395,7 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
     const int64_t max_slabs_per_lor = (int64_t)sp.slabs_pf * sp.nbands;
     const size_t budget = (size_t)g_seg_scratch_bytes.load(std::memory_order_relaxed);
     int64_t chunk = (int64_t)(budget / (sizeof(int) * (size_t)max_slabs_per_lor +
-                                        sizeof(LorRec) + sizeof(int)));
+                                        (p.gen ? 0 : sizeof(LorRec)) + sizeof(int)));
     chunk = std::max<int64_t>(kSegTile, chunk / kSegTile * kSegTile);
     chunk = std::min<int64_t>(chunk, p.n);
     sp.ntiles = (int)((chunk + kSegTile - 1) / kSegTile);
@@ -1224,7 +1407,7 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
     const size_t b_offs = al(sizeof(int64_t) * (size_t)sp.ntiles * sp.n_slabs);
     const size_t b_slab = al(sizeof(int64_t) * (2 * sp.n_slabs + 1));
     const size_t b_seg = al(sizeof(int) * cap);
-    const size_t b_rec = al(sizeof(LorRec) * chunk);
+    const size_t b_rec = p.gen ? 0 : al(sizeof(LorRec) * chunk);  // generated: none
     char *ws = nullptr;
     cudaError_t e = scratch_alloc((void **)&ws,
                                   b_rec + b_range + b_counts + b_offs + b_slab + b_seg, stream);
@@ -1232,7 +1415,7 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
         set_cuda_error(e);
         return SRF_ERR_CUDA;
     }
-    sp.rec = reinterpret_cast<LorRec *>(ws);
+    sp.rec = p.gen ? nullptr : reinterpret_cast<LorRec *>(ws);
     char *w2 = ws + b_rec;
     sp.range = reinterpret_cast<int *>(w2);
     sp.tile_counts = reinterpret_cast<int *>(w2 + b_range);
@@ -1473,6 +1656,45 @@ extern "C" int srf_tor_maplors(const float *x1, const float *y1, const float *z1
     p.geo = geo_sigma2_flag != 0;
     p.values = projection_value;
     p.image_out = image;
+    return tor_launch<kMap>(p, (cudaStream_t)stream);
+}
+
+extern "C" int srf_tor_maplors_generated(int kind, const float *crystals, int n_rings,
+                                         int n_blocks, int n_per_block,
+                                         unsigned long long seed, int64_t first,
+                                         int64_t count, int axis, int geo_sigma2_flag,
+                                         const int *grid, const float *center,
+                                         const float *size, float kernel_width, float *image,
+                                         int accumulate, void *stream) {
+    if (kind != 0 && kind != 1) return SRF_ERR_INVALID_ARGUMENT;
+    if (axis < 0 || axis > 2 || first < 0 || count < 0) return SRF_ERR_INVALID_ARGUMENT;
+    if (n_rings < 1 || n_blocks < 1 || n_per_block < 1) return SRF_ERR_INVALID_ARGUMENT;
+    const int64_t n_cry = (int64_t)n_rings * n_blocks * n_per_block;
+    if (n_cry < 2 || n_cry > ((int64_t)1 << 31) - 1) return SRF_ERR_INVALID_ARGUMENT;
+    if (kind == 1) {
+        if (n_blocks < 2) return SRF_ERR_INVALID_ARGUMENT;
+        const double cb = (double)n_per_block * n_per_block;
+        const double total = (double)n_rings * ((double)(n_rings - 1) * n_blocks *
+                                                (n_blocks - 1) * cb +
+                                                (double)n_blocks * (n_blocks - 1) / 2 * cb);
+        if ((double)first + (double)count > total) return SRF_ERR_INVALID_ARGUMENT;
+    }
+    TorParams p{};
+    int st = tor_setup(p, grid, center, size, kernel_width, 0.0f, 1.0e30f, count, 1);
+    if (st != SRF_OK) return st;
+    if (!image || (count > 0 && !crystals)) return SRF_ERR_INVALID_ARGUMENT;
+    if (!accumulate && (st = zero_image(image, grid, (cudaStream_t)stream)) != SRF_OK) return st;
+    p.geo = geo_sigma2_flag != 0;
+    p.values = nullptr;  // every LOR's value is 1
+    p.image_out = image;
+    p.gen = kind + 1;
+    p.gen_axis = axis;
+    p.gen_first = first;
+    p.gen_seed = seed;
+    p.crystals = crystals;
+    p.n_rings = n_rings;
+    p.n_blocks = n_blocks;
+    p.n_per_block = n_per_block;
     return tor_launch<kMap>(p, (cudaStream_t)stream);
 }
 

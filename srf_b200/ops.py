@@ -220,6 +220,28 @@ def tor_maplors(image, grid, center, size, lors, lors_value, kernel_width,
     return res
 
 
+
+def tor_maplors_generated(kind, crystals, n_rings, n_blocks, n_per_block, seed, first, count,
+                          axis, grid, center, size, kernel_width, geo_sigma2_flag=False,
+                          out=None, accumulate=False):
+    """Maplors of generated detector-pair LORs ``first .. first+count-1`` of dominant-axis
+    group ``axis`` (0, 1, 2) into an image in that group's kernel layout
+    (``srf_tor_maplors_generated``: kind 0 random crystal pairs, kind 1 the scanner's
+    block-pair enumeration). ``crystals``: CUDA float32 [n_crystals, 3]."""
+    dev = _check_cuda(crystals, out)
+    if crystals.dtype != torch.float32 or not crystals.is_contiguous() or crystals.dim() != 2 \
+            or crystals.shape[1] != 3:
+        raise ValueError("crystals must be a contiguous float32 [n, 3] CUDA tensor")
+    g, ga, ca, sa = _geom(grid, center, size)
+    res, _ = _out_image(out, g, crystals)
+    with torch.cuda.device(dev):
+        _call(dev, "srf_tor_maplors_generated", int(kind), crystals.data_ptr(), int(n_rings),
+              int(n_blocks), int(n_per_block), int(seed) & ((1 << 64) - 1), int(first),
+              int(count), int(axis), int(bool(geo_sigma2_flag)), ga, ca, sa,
+              float(kernel_width), res.data_ptr(),
+              int(bool(accumulate) and out is not None), _stream(dev))
+    return res
+
 def tor_count_samples(lors, grid, center, size, kernel_width, geo_sigma2_flag=False,
                       layout="auto"):
     """Per-LOR (non-zero-weight voxels, window voxels visited) as int32 [2, N]: the

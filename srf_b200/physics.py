@@ -243,3 +243,20 @@ def map_lors(model, data, image):
     if isinstance(model, CompleteLoRsModel) and not isinstance(data, ListModeDataWithoutTOF):
         data = ListModeDataWithoutTOF(data.lors, data.values)
     return backprojection(model, data, image)
+
+
+def map_generated(model, pairs, image, first=0, count=None):
+    """Maplors of generated detector-pair LORs ``first .. first+count-1``
+    (``synthetic.GeneratedPairs``) for the TOR model, with no LOR array in memory: per
+    axis group one ``srf_tor_maplors_generated`` call, then the reference's transpose back
+    and sum (split_lors.py:116-133). Returns an ``Image`` in the input image's layout."""
+    if not isinstance(model, SplitLoRsModel):
+        raise TypeError("generated LORs are mapped by the TOR model")
+    count = len(pairs) - first if count is None else count
+    parts = []
+    for k, a in enumerate(model.AXIS):
+        _, g, c, s = model.kernel_geometry(image, a)
+        parts.append((a, ops.tor_maplors_generated(
+            pairs.kind, pairs.crystals, pairs.n_rings, pairs.n_blocks, pairs.n_per_block,
+            pairs.seed, first, count, k, g, c, s, model.kernel_width, model.geo_sigma2_flag)))
+    return _sum_back(model, parts, image)

@@ -8,10 +8,11 @@ kernel Pz [nz, nz] and a sparse transaxial kernel Axy [nx*ny, nx*ny]:
     psf(X)      = Axy (X Pz^T)        (recon_step.py:78-87)
     psf^T(B)    = Axy^T (B Pz)        (recon_step.py:95-101)
 
-and one step is x <- update(x, psf^T(backprojection(projection(psf(x)))), effmap). The
-axial product is a plain library GEMM (nz is small); the sparse product is the library's
-CSR kernel (``srf_csr_spmm``: a warp per row of Axy, lanes over z), with Axy^T built once
-on the host.
+and one step is x <- update(x, psf^T(backprojection(projection(psf(x)))), effmap). Each
+application is one launch of the library's fused kernel (``srf_psf_apply``): a warp per
+row of Axy sums its neighbours' rows of X (lanes over z), then multiplies that row by
+Pz^T (or Pz) held in shared memory, so no intermediate [nx*ny, nz] matrix is written.
+Axy^T is built once on the host for the adjoint.
 """
 
 import numpy as np
@@ -48,12 +49,14 @@ class PSF:
         if self.fwd[3][0] != self.fwd[3][1]:
             raise ValueError("psf_xy must be a square [nx*ny, nx*ny] matrix")
 
-    def _spmm(self, csr, x):
+    def _psf(self, csr, x, transpose_pz):
+        """csr (x Pz^T) (transpose_pz = 0) or csr (x Pz) (1), x a contiguous [rows, nz]."""
         rowptr, col, val, shape = csr
         y = torch.empty((shape[0], x.shape[1]), dtype=torch.float32, device=x.device)
         with torch.cuda.device(x.device):
-            _lib.call("srf_csr_spmm", rowptr.data_ptr(), col.data_ptr(), val.data_ptr(),
-                      shape[0], shape[1], x.data_ptr(), x.shape[1], y.data_ptr(), 0,
+            _lib.call("srf_psf_apply", rowptr.data_ptr(), col.data_ptr(), val.data_ptr(),
+                      shape[0], shape[1], x.data_ptr(), x.shape[1], self.pz.data_ptr(),
+                      int(transpose_pz), y.data_ptr(), 0,
                       torch.cuda.current_stream(x.device).cuda_stream)
         return y
 
@@ -65,17 +68,17 @@ class PSF:
         return nx, ny, nz
 
     def apply(self, image):
-        """psf(image): Axy (X Pz^T), as an Image."""
+        """psf(image): Axy (X Pz^T) (recon_step.py:78-87), as an Image."""
         nx, ny, nz = self._check(image.data)
-        x = image.data.reshape(nx * ny, nz) @ self.pz.t()
-        out = self._spmm(self.fwd, x.contiguous()).reshape(nx, ny, nz)
+        x = image.data.reshape(nx * ny, nz).contiguous()
+        out = self._psf(self.fwd, x, 0).reshape(nx, ny, nz)
         return Image(out, image.center, image.size)
 
     def adjoint(self, image):
-        """psf^T(image): Axy^T (B Pz), as an Image."""
+        """psf^T(image): Axy^T (B Pz) (recon_step.py:95-101), as an Image."""
         nx, ny, nz = self._check(image.data)
-        b = image.data.reshape(nx * ny, nz) @ self.pz
-        out = self._spmm(self.adj, b.contiguous()).reshape(nx, ny, nz)
+        b = image.data.reshape(nx * ny, nz).contiguous()
+        out = self._psf(self.adj, b, 1).reshape(nx, ny, nz)
         return Image(out, image.center, image.size)
 
 

@@ -29,7 +29,8 @@ import torch
 
 from . import ops
 from .data import Image, ListModeData, ListModeDataSplit
-from .physics import CompleteLoRsModel, SplitLoRsModel, map_lors, projection_backprojection
+from .physics import (CompleteLoRsModel, SplitLoRsModel, map_generated, map_lors,
+                      projection_backprojection)
 from .preprocess import crop_mask, map_process, merge_effmap, split_listmode
 
 
@@ -100,6 +101,54 @@ def order_subset(model, data, image):
 # ---------------------------------------------------------------------- efficiency map
 
 
+def _chunk_reader(lors, chunk):
+    """(n, chunk, device, take(start, count)) of an [N, 6] tensor or a chunked source."""
+    if callable(lors):
+        return (len(lors), getattr(lors, "chunk", chunk),
+                getattr(lors, "device", torch.device("cuda")), lors)
+    return lors.shape[0], chunk, lors.device, (lambda s, c: lors[s:s + c])
+
+
+def map_chunk_default(model, part, img, order=True):
+    """Maplors of one chunk of [count, 6] detector-pair LORs into ``img``'s geometry
+    (``map_process`` and the axis groups for the TOR model, the raw LORs for Siddon)."""
+    if isinstance(model, SplitLoRsModel):
+        groups = map_process(part)
+        if order:
+            from .preprocess import order_by_direction
+            groups = order_by_direction(groups)
+        data = split_listmode(groups, without_tof=True)
+    else:
+        from .data import ListModeDataWithoutTOF
+        data = ListModeDataWithoutTOF(part, torch.ones(part.shape[0], device=part.device))
+    return map_lors(model, data, img).data
+
+
+def map_sum(model, lors, grid, center, size, chunk=16_000_000, order=True, chunks=None,
+            map_chunk=None):
+    """Sum of Maplors over the chunks of ``lors`` (before the crop / normalise / invert
+    of ``merge_effmap``). ``chunks``: indices of the chunks to take (all by default; a
+    rank of a sharded pass takes its own); ``map_chunk(model, part, img)`` maps one chunk
+    (``map_chunk_default``)."""
+    from .synthetic import GeneratedPairs
+    n, chunk, dev, take = _chunk_reader(lors, chunk)
+    total = torch.zeros(tuple(grid), dtype=torch.float32, device=dev)
+    img = Image(total, center, size)
+    fused = isinstance(lors, GeneratedPairs) and isinstance(model, SplitLoRsModel) \
+        and map_chunk is None
+    fn = map_chunk or (lambda m, part, im: map_chunk_default(m, part, im, order))
+    n_chunks = (n + chunk - 1) // chunk
+    for c in (range(n_chunks) if chunks is None else chunks):
+        s = c * chunk
+        if s >= n:
+            continue
+        if fused:  # the kernels make the LORs themselves: nothing is materialised
+            total.add_(map_generated(model, lors, img, s, min(chunk, n - s)).data)
+        else:
+            total.add_(fn(model, take(s, min(chunk, n - s)), img))
+    return total
+
+
 def efficiency_map(model, lors, grid, center, size, inner_radius, axial_length,
                    chunk=16_000_000, crop_ratio=0.95, threshold=1e-6, zero_below=True,
                    order=True):
@@ -108,34 +157,14 @@ def efficiency_map(model, lors, grid, center, size, inner_radius, axial_length,
     (merge_map.py:37-41). ``lors`` is an [N, 6] CUDA tensor, or a source with ``len()``
     and ``source(start, count)`` returning [count, 6] CUDA chunks (for example
     ``synthetic.RandomLorSource``), so that N LORs never exist at once; its chunk size
-    then sets ``chunk``. With ``order`` (TOR model) each chunk's map records are
+    then sets ``chunk``. A ``synthetic.GeneratedPairs`` source with the TOR model is
+    mapped by kernels that make each LOR from its number: no LOR array at all. With ``order`` (TOR model) each chunk's map records are
     reordered by direction inside 4096-record blocks (``preprocess.order_by_direction``)
     before Maplors: the map is the same sum taken in another order, and the slab kernels
     walk fewer voxel slots for LORs of mixed directions (random detector pairs)."""
-    if callable(lors):
-        n = len(lors)
-        chunk = getattr(lors, "chunk", chunk)
-        dev = getattr(lors, "device", torch.device("cuda"))
-        take = lors
-    else:
-        n = lors.shape[0]
-        dev = lors.device
-        take = lambda s, c: lors[s:s + c]  # noqa: E731
-    total = torch.zeros(tuple(grid), dtype=torch.float32, device=dev)
-    img = Image(total, center, size)
-    for s in range(0, n, chunk):
-        part = take(s, min(chunk, n - s))
-        if isinstance(model, SplitLoRsModel):
-            groups = map_process(part)
-            if order:
-                from .preprocess import order_by_direction
-                groups = order_by_direction(groups)
-            data = split_listmode(groups, without_tof=True)
-        else:
-            from .data import ListModeDataWithoutTOF
-            data = ListModeDataWithoutTOF(part, torch.ones(part.shape[0], device=dev))
-        total.add_(map_lors(model, data, img).data)
-    keep = crop_mask(grid, center, size, inner_radius, axial_length, crop_ratio, device=dev)
+    total = map_sum(model, lors, grid, center, size, chunk, order)
+    keep = crop_mask(grid, center, size, inner_radius, axial_length, crop_ratio,
+                     device=total.device)
     return Image(merge_effmap(total, keep, threshold, zero_below), center, size), total
 
 

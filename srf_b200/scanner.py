@@ -107,6 +107,13 @@ class CylindricalPET:
                         [0.0, 0.0, 1.0]])
         return (rot @ m).T
 
+    def crystal_table(self):
+        """[nb_rings * nb_blocks_per_ring * crystals per block, 3] float32 crystal centres,
+        ring major, then block, then the block's mesh order (``block_meshes``): the table
+        the generated block-pair LORs index (``synthetic.GeneratedPairs.block_pairs``)."""
+        return np.vstack([self.block_meshes(ir, ib) for ir in range(self.nb_rings)
+                          for ib in range(self.nb_blocks_per_ring)]).astype(np.float32)
+
     @staticmethod
     def block_pairs(n_blocks, same_ring):
         """Block index pairs of ``make_block_pairs`` (scanner/pet/pet.py:149-168)."""

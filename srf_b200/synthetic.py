@@ -211,6 +211,104 @@ def random_lors(n, scanner, seed, device="cpu"):
     return torch.cat([pos[i], pos[j]], 1).contiguous()
 
 
+_GAMMA = 0x9E3779B97F4A7C15
+_MASK64 = (1 << 64) - 1
+
+
+def splitmix64(seed, k):
+    """SplitMix64 output number ``k`` (numpy uint64 array) of the stream seeded ``seed``
+    (Steele, Lea and Flood, OOPSLA 2014): the finaliser of seed + (k + 1) * gamma. The
+    host mirror of the generator in the TOR map kernels (``srf_tor_maplors_generated``)."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed & _MASK64) + (np.asarray(k, np.uint64) + np.uint64(1)) * np.uint64(_GAMMA)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def random_pair_indices(n_crystals, seed, first, count):
+    """Crystal indices (a, b) of generated random pairs first .. first+count-1: the host
+    mirror of kind 0 of ``srf_tor_maplors_generated`` (a = floor(u1 n / 2^32), b =
+    floor(u2 (n - 1) / 2^32) shifted up past a, (u1, u2) the halves of SplitMix64)."""
+    h = splitmix64(seed, np.arange(first, first + count, dtype=np.uint64))
+    u1, u2 = h >> np.uint64(32), h & np.uint64(0xFFFFFFFF)
+    n = np.uint64(n_crystals)
+    a = ((u1 * n) >> np.uint64(32)).astype(np.int64)
+    j = ((u2 * (n - np.uint64(1))) >> np.uint64(32)).astype(np.int64)
+    return a, j + (j >= a)
+
+
+class GeneratedPairs:
+    """Detector-pair LORs that the TOR map kernels make on the fly from their number, so
+    that no LOR array exists at any point (``srf_tor_maplors_generated``):
+
+    * ``GeneratedPairs.random(scanner, n, seed)``: n uniform pairs of distinct crystals
+      (SplitMix64, see ``random_pair_indices``);
+    * ``GeneratedPairs.block_pairs(cylindrical_pet)``: every crystal pair of the scanner's
+      block pairs over all ring pairs, in the reference's effmap order
+      (srfapp_new.py:153-157, scanner/pet/pet.py:149-177).
+
+    ``crystals`` (float32 [n, 3]) is uploaded once; ``host_lors(first, count)`` returns the
+    same LORs as a numpy [count, 6] array (for checks and for models without the fused
+    path)."""
+
+    def __init__(self, kind, crystals, n, seed=0, n_rings=1, n_blocks=1, n_per_block=None,
+                 chunk=1 << 26, device="cuda"):
+        self.kind = int(kind)
+        self.host_crystals = np.ascontiguousarray(crystals, np.float32)
+        self.n = int(n)
+        self.seed = int(seed)
+        self.n_rings, self.n_blocks = int(n_rings), int(n_blocks)
+        self.n_per_block = int(n_per_block if n_per_block is not None
+                               else len(self.host_crystals) // (self.n_rings * self.n_blocks))
+        self.chunk = int(chunk)
+        self.device = torch.device(device)
+        self.crystals = torch.as_tensor(self.host_crystals, device=self.device)
+
+    @classmethod
+    def random(cls, scanner, n, seed, chunk=1 << 26, device="cuda"):
+        pos = scanner.crystal_positions()
+        return cls(0, pos, n, seed, 1, 1, len(pos), chunk, device)
+
+    @classmethod
+    def block_pairs(cls, pet, chunk=1 << 26, device="cuda"):
+        table = pet.crystal_table()
+        nr, nb = pet.nb_rings, pet.nb_blocks_per_ring
+        ncb = len(table) // (nr * nb)
+        cb = ncb * ncb
+        n = nr * ((nr - 1) * nb * (nb - 1) * cb + nb * (nb - 1) // 2 * cb)
+        return cls(1, table, n, 0, nr, nb, ncb, chunk, device)
+
+    def __len__(self):
+        return self.n
+
+    def pair_indices(self, first, count):
+        """(a, b) crystal indices of LORs first .. first+count-1 (host)."""
+        if self.kind == 0:
+            return random_pair_indices(len(self.host_crystals), self.seed, first, count)
+        nr, nb, ncb = self.n_rings, self.n_blocks, self.n_per_block
+        a_all, b_all = [], []
+        for ir1 in range(nr):
+            for ir2 in range(nr):
+                for i1 in range(nb):
+                    for i2 in range(nb):
+                        if (ir1 == ir2 and i1 < i2) or (ir1 != ir2 and i1 != i2):
+                            c1 = (ir1 * nb + i1) * ncb + np.repeat(np.arange(ncb), ncb)
+                            c2 = (ir2 * nb + i2) * ncb + np.tile(np.arange(ncb), ncb)
+                            a_all.append(c1)
+                            b_all.append(c2)
+        a, b = np.concatenate(a_all), np.concatenate(b_all)
+        return a[first:first + count], b[first:first + count]
+
+    def host_lors(self, first, count):
+        a, b = self.pair_indices(first, count)
+        return np.hstack([self.host_crystals[a], self.host_crystals[b]])
+
+    def __call__(self, start, count):
+        """[count, 6] LORs on the device (materialised: models without the fused path)."""
+        return torch.as_tensor(self.host_lors(start, count), device=self.device)
+
+
 class RandomLorSource:
     """Random detector-pair LORs generated on the device chunk by chunk: chunk k of
     ``chunk`` LORs is ``random_lors(count, scanner, seed * 1000003 + k)``, so any chunk

@@ -464,3 +464,44 @@ def test_effmap_record_order_changes_only_summation_order():
     assert torch.count_nonzero(b) > 0
     assert float((a - b).norm() / b.norm()) < 1e-6
     assert float((ea.data - eb.data).norm() / eb.data.norm()) < 1e-5
+
+
+# ------------------------------------------------------ sharded drivers on one rank
+
+
+def test_sharded_drivers_on_one_rank_run_the_library_path(prob):
+    """With no process group (one rank) the sharded drivers run the library's GPU path
+    and equal the single-process drivers: ShardedOSEM = recon.OSEM (eager and graph),
+    sharded_efficiency_map = recon.efficiency_map, ShardedBatchedOSEM = BatchedOSEM."""
+    from srf_b200 import parallel
+    from srf_b200.batched import BatchedOSEM
+    from srf_b200.synthetic import RandomLorSource
+    case, model, data, eff = prob
+    x0 = Image(cu(case["image"]) + 0.5, case["center"], case["size"])
+    e = Image(cu(eff), case["center"], case["size"])
+    for use_graph in (False, True):
+        a = parallel.ShardedOSEM(model, data, e, x0, n_subsets=4, use_graph=use_graph)
+        b = recon.OSEM(model, data, e, x0, n_subsets=4)
+        a.step(), a.step(), b.step(), b.step()
+        assert K.rel_l2(a.x.data.cpu().numpy(), b.x.data.cpu().numpy()) < 1e-6
+        a.release()
+
+    grid, voxel = (32, 32, 16), 6.4
+    size = [g * voxel for g in grid]
+    src = RandomLorSource(250_000, K.SCANNER, 5, chunk=100_000)
+    args = (list(grid), [0, 0, 0], size, K.SCANNER.inner_radius, K.SCANNER.axial_length)
+    inv_a, tot_a = parallel.sharded_efficiency_map(model, src, *args)
+    inv_b, tot_b = recon.efficiency_map(model, src, *args)
+    assert torch.count_nonzero(tot_b) > 0
+    assert float((tot_a - tot_b).norm() / tot_b.norm()) < 1e-6
+
+    frames, fgrid, fsize = _frames(4, 2)
+    feff = Image(cu(np.full(fgrid, 0.9, np.float32)), [0, 0, 0], fsize)
+    fx0 = cu(np.ones(fgrid, np.float32))
+    sb = parallel.ShardedBatchedOSEM(model, frames, feff, fx0, n_subsets=2)
+    bb = BatchedOSEM(model, frames, feff, fx0, n_subsets=2)
+    sb.step(), bb.step()
+    imgs = sb.images()
+    assert sorted(imgs) == list(range(4))
+    for f in range(4):
+        assert K.rel_l2(imgs[f].cpu().numpy(), bb.x[f].cpu().numpy()) < 1e-6

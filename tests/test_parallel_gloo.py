@@ -112,3 +112,144 @@ def test_sharded_mlem_two_ranks_equals_single_process():
         num = np.linalg.norm(out[r] - ref)
         assert num / np.linalg.norm(ref) < 1e-6, r
     np.testing.assert_array_equal(out[0], out[1])  # every rank holds the same image
+
+
+# ------------------------------------------------------------- sharded OSEM, effmap, frames
+
+
+def oracle_project_back(model, image, data):
+    proj = oracle_projection(model, image, data)
+    return proj, oracle_backprojection(model, proj, image)
+
+
+def cpu_update(x, effinv, bp):
+    x.mul_(effinv * bp)
+
+
+def _osem_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from srf_b200.parallel import ShardedOSEM
+        model, data, effinv, x0 = _problem()
+        m = ShardedOSEM(model, data, effinv, x0, n_subsets=3,
+                        project_back=oracle_project_back, update=cpu_update)
+        m.step()
+        q.put((rank, m.step().data.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def _spawn(target, world=2):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=target, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in procs:
+        r, x = q.get(timeout=300)
+        out[r] = x
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return out
+
+
+def test_subset_shards_partition_the_subsets():
+    """Over the ranks, the parts of subset k are exactly recon.make_subsets' subset k."""
+    from srf_b200.parallel import subset_shard
+    from srf_b200.recon import make_subsets
+    for n in (0, 1, 5, 17, 64):
+        data = ListModeData(torch.arange(n, dtype=torch.float32)[:, None].repeat(1, 3),
+                            torch.arange(n, dtype=torch.float32))
+        for S in (1, 2, 3, 4):
+            full = make_subsets(data, S)
+            for W in (1, 2, 3):
+                for k in range(S):
+                    got = torch.cat([subset_shard(data, k, S, r, W).values for r in range(W)])
+                    assert torch.equal(torch.sort(got).values, full[k].values), (n, S, W, k)
+
+
+def test_sharded_osem_two_ranks_equals_single_process():
+    from srf_b200.parallel import ShardedOSEM
+    model, data, effinv, x0 = _problem()
+    single = ShardedOSEM(model, data, effinv, x0, n_subsets=3,
+                         project_back=oracle_project_back, update=cpu_update)
+    single.step()
+    ref = single.step().data.numpy()
+    out = _spawn(_osem_worker)
+    for r in range(2):
+        assert np.linalg.norm(out[r] - ref) / np.linalg.norm(ref) < 1e-6, r
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+class _PairSource:
+    """A small chunked detector-pair source on the CPU (the random_lors generator)."""
+    chunk = 250
+    device = torch.device("cpu")
+
+    def __len__(self):
+        return 1100
+
+    def __call__(self, start, count):
+        from srf_b200.scanner import RingScanner
+        from srf_b200.synthetic import random_lors
+        return random_lors(count, RingScanner(400.0, 400, 32, 3.2), 11 + start // self.chunk)
+
+
+def oracle_map_chunk(model, part, img):
+    """Maplors of one chunk by the oracle: numpy map_process, then tor_maplors per axis."""
+    groups = P.map_process(part.numpy().astype(np.float32))
+    total = np.zeros(img.data.shape, np.float64)
+    for a in model.AXIS:
+        lors = np.ascontiguousarray(groups[a].astype(np.float32).T)
+        if lors.shape[1] == 0:
+            continue
+        _, g, c, s = P.axis_view(img.data.numpy(), img.center, img.size, a)
+        m = O.tor_maplors(lors, np.ones(lors.shape[1], np.float32), g, c, s,
+                          model.kernel_width, model.geo_sigma2_flag)
+        total += np.transpose(m, model.perm_back(a))
+    return torch.as_tensor(total.astype(np.float32))
+
+
+_MAP_GEOM = ((16, 16, 8), [0.0, 0.0, 0.0], [409.6, 409.6, 204.8])
+
+
+def _map_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from srf_b200.parallel import sharded_efficiency_map
+        model, _, _, _ = _problem()
+        grid, center, size = _MAP_GEOM
+        inv, total = sharded_efficiency_map(model, _PairSource(), grid, center, size, 400.0,
+                                            102.4, map_chunk=oracle_map_chunk)
+        q.put((rank, (inv.data.numpy(), total.numpy())))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_efficiency_map_two_ranks_equals_single_process():
+    from srf_b200.recon import map_sum
+    from srf_b200.preprocess import crop_mask, merge_effmap
+    model, _, _, _ = _problem()
+    grid, center, size = _MAP_GEOM
+    ref = map_sum(model, _PairSource(), grid, center, size, map_chunk=oracle_map_chunk)
+    assert float(ref.sum()) > 0
+    ref_inv = merge_effmap(ref, crop_mask(grid, center, size, 400.0, 102.4, device="cpu"))
+    out = _spawn(_map_worker)
+    for r in range(2):
+        inv, total = out[r]
+        assert np.linalg.norm(total - ref.numpy()) / np.linalg.norm(ref.numpy()) < 1e-6
+        assert np.linalg.norm(inv - ref_inv.numpy()) / np.linalg.norm(ref_inv.numpy()) < 1e-5
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
+def test_shard_frames_cover_every_frame_once():
+    from srf_b200.parallel import shard_frames
+    for n in (0, 1, 7, 64):
+        for w in (1, 2, 3, 8):
+            got = sorted(f for r in range(w) for f in shard_frames(n, r, w))
+            assert got == list(range(n))

@@ -1,6 +1,7 @@
-"""PSF reconstruction step: the separable PSF against a dense numpy computation, its
-adjoint identity, the loader (MATLAB + .npy files), and the step with an identity PSF equal
-to the plain reconstruction step."""
+"""PSF reconstruction step: the fused PSF kernel against the numpy restatement of
+recon_step.py:78-87 / :95-101 (oracle, float32 and float64), its adjoint identity, the
+loader (MATLAB + .npy files), and the step with an identity PSF equal to the plain
+reconstruction step."""
 
 import numpy as np
 import pytest
@@ -43,8 +44,10 @@ def test_load_psf_files(tmp_path):
 
 
 @pytest.mark.gpu
-def test_psf_matches_dense_and_is_adjoint():
-    nx, ny, nz = 16, 12, 8
+@pytest.mark.parametrize("shape", [(16, 12, 8), (20, 18, 64), (9, 7, 130)])
+def test_psf_matches_the_oracle_and_is_adjoint(shape):
+    from oracle import preprocess_ref as P
+    nx, ny, nz = shape
     xy, z = _psf_mats(nx, ny, nz)
     p = PSF(xy, z)
     rng = np.random.default_rng(4)
@@ -53,16 +56,34 @@ def test_psf_matches_dense_and_is_adjoint():
     from srf_b200.data import Image
     X = Image(torch.as_tensor(x).cuda(), [0, 0, 0], [1, 1, 1])
     Y = Image(torch.as_tensor(yv).cuda(), [0, 0, 0], [1, 1, 1])
-    A = xy.toarray().astype(np.float64)
-    ref = (A @ (x.reshape(nx * ny, nz).astype(np.float64) @ z.T.astype(np.float64)))
-    got = p.apply(X).data.cpu().numpy().reshape(nx * ny, nz)
-    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-6
-    refa = A.T @ (yv.reshape(nx * ny, nz).astype(np.float64) @ z.astype(np.float64))
-    gota = p.adjoint(Y).data.cpu().numpy().reshape(nx * ny, nz)
-    assert np.linalg.norm(gota - refa) / np.linalg.norm(refa) < 1e-6
+    A32 = xy.tocsr().astype(np.float32)
+    A64 = xy.tocsr().astype(np.float64)
+    got = p.apply(X).data.cpu().numpy()
+    gota = p.adjoint(Y).data.cpu().numpy()
+
+    def rel(a, b):
+        return float(np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(b))
+
+    # float32: the reference's product order; float64: the exact value
+    assert rel(got, P.psf_forward(A32, z, x)) < 1e-6
+    assert rel(got, P.psf_forward(A64, z.astype(np.float64), x.astype(np.float64))) < 1e-6
+    assert rel(gota, P.psf_adjoint(A32, z, yv)) < 1e-6
+    assert rel(gota, P.psf_adjoint(A64, z.astype(np.float64), yv.astype(np.float64))) < 1e-6
     lhs = float((p.apply(X).data.double() * Y.data.double()).sum())
     rhs = float((X.data.double() * p.adjoint(Y).data.double()).sum())
     assert abs(lhs - rhs) / abs(lhs) < 1e-6
+
+
+def test_psf_oracle_restatement_is_separable():
+    """The oracle's product order (dense axial first) equals the other association."""
+    from oracle import preprocess_ref as P
+    xy, z = _psf_mats(5, 4, 6)
+    x = np.random.default_rng(1).random((5, 4, 6))
+    A = xy.toarray()
+    np.testing.assert_allclose(P.psf_forward(xy.tocsr(), z.astype(np.float64), x),
+                               ((A @ x.reshape(20, 6)) @ z.T).reshape(5, 4, 6), rtol=1e-12)
+    np.testing.assert_allclose(P.psf_adjoint(xy.tocsr(), z.astype(np.float64), x),
+                               ((A.T @ x.reshape(20, 6)) @ z).reshape(5, 4, 6), rtol=1e-12)
 
 
 @pytest.mark.gpu
