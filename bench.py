@@ -94,6 +94,11 @@ def parse_args(argv=None):
     ap.add_argument("--no-variants", dest="variants", action="store_false",
                     help="skip the config variants of the same step (the reference preset "
                          "kernel_width 4.0; the geometric sigma2 factor on)")
+    ap.add_argument("--effmap-source", default="tensor", choices=["generated", "tensor"],
+                    help="effmap LORs: generated per chunk as a tensor, preprocessed and "
+                         "ordered by direction (tensor, the default: the faster path), or "
+                         "made inside the map kernels from their number with no LOR array "
+                         "(generated)")
     ap.add_argument("--tuning", default=None,
                     help="PATH,SLAB_SLICES,GRID_MULT for srf_tor_set_tuning, or PATH for "
                          "srf_siddon_set_tuning with --workload siddon64 (default: the "
@@ -166,6 +171,16 @@ def _image_of(t, wl):
     return Image(t, wl.center, wl.size)
 
 
+def effmap_source(args, wl, n, seed, dev):
+    """The effmap's detector-pair source for ``--effmap-source``: LORs made inside the map
+    kernels (``GeneratedPairs``), or generated per 16M chunk as a tensor
+    (``RandomLorSource``)."""
+    from srf_b200 import synthetic as S
+    if args.effmap_source == "generated":
+        return S.GeneratedPairs.random(wl.scanner, n, seed, device=dev)
+    return S.RandomLorSource(n, wl.scanner, seed, device=dev)
+
+
 def run_large_recon(args):
     """The large axial FOV reconstruction end to end: 200M seeded TOF events (400 ps) from
     the multi-cylinder phantom, streamed in 16M-event chunks from pinned host memory
@@ -221,11 +236,10 @@ def run_large_recon(args):
     data = PP.split_listmode(groups)
     args_e = (list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
               wl.scanner.axial_length)
-    recon.efficiency_map(model, S.RandomLorSource(chunk, wl.scanner, 78, device=dev),
-                         *args_e, order=args.order)  # warm-up: one chunk (sizes the scratch pool)
+    recon.efficiency_map(model, effmap_source(args, wl, chunk, 78, dev), *args_e,
+                         order=args.order)  # warm-up: one chunk (sizes the scratch pool)
     (effinv, _), effmap_ms = timed(lambda: recon.efficiency_map(
-        model, S.RandomLorSource(wl.n_effmap, wl.scanner, 77, device=dev), *args_e,
-        order=args.order))
+        model, effmap_source(args, wl, wl.n_effmap, 77, dev), *args_e, order=args.order))
     x0 = _image_of(initial_image(list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
                                  wl.scanner.axial_length, dev), wl)
     osem, setup_ms = timed(lambda: recon.OSEM(model, data, effinv, x0, n_subsets=wl.subsets))
@@ -247,7 +261,7 @@ def run_large_recon(args):
                        "voxel_mm": wl.voxel, "tof_res_ps": wl.tof_res_ps,
                        "kernel_width": round(wl.kernel_width, 4), "chunk_events": chunk,
                        "iterations": wl.iterations, "subsets": wl.subsets,
-                       "effmap_lors": wl.n_effmap},
+                       "effmap_lors": wl.n_effmap, "effmap_source": args.effmap_source},
             "path": "per chunk: pinned host events -> device -> recon_process; effmap: "
                     "on-device random pairs -> map_process -> maplors; OSEM: subsets split "
                     "and ordered once, then per subset one combined projection + "
@@ -1156,12 +1170,11 @@ def main(argv=None):
     effmap = osem = None
     if args.effmap:
         from srf_b200 import recon
-        from srf_b200.synthetic import RandomLorSource
         args_e = (list(wl.grid), wl.center, wl.size, wl.scanner.inner_radius,
                   wl.scanner.axial_length)
-        recon.efficiency_map(model, RandomLorSource(16_000_000, wl.scanner, 78, device=dev),
-                             *args_e, order=args.order)  # warm-up: one full chunk
-        src = RandomLorSource(wl.n_effmap, wl.scanner, 77, device=dev)
+        recon.efficiency_map(model, effmap_source(args, wl, 16_000_000, 78, dev), *args_e,
+                             order=args.order)  # warm-up: one full chunk
+        src = effmap_source(args, wl, wl.n_effmap, 77, dev)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -1171,10 +1184,25 @@ def main(argv=None):
         e_ms = max_over_ranks(e0.elapsed_time(e1), world)
         effmap = {"lors": wl.n_effmap, "ms": e_ms, "lors_per_s": wl.n_effmap / (e_ms / 1e3),
                   "chunk": src.chunk,
-                  "path": "random crystal pairs generated on the device per chunk -> "
-                          "map_process -> " + ("records ordered by direction -> "
-                                               if args.order else "")
-                          + "TOR maplors of each axis group -> crop, normalise, invert"}
+                  "source": args.effmap_source,
+                  "path": ("random crystal pairs (SplitMix64) made inside the binning and map "
+                           "kernels from each LOR's number, map_process per LOR, no LOR array "
+                           "-> TOR maplors of each axis group -> crop, normalise, invert"
+                           if args.effmap_source == "generated" else
+                           "random crystal pairs generated on the device per chunk -> "
+                           "map_process -> " + ("records ordered by direction -> "
+                                                if args.order else "")
+                           + "TOR maplors of each axis group -> crop, normalise, invert")}
+        if args.effmap_source == "tensor":
+            # the same pass with LORs made inside the map kernels (no LOR array)
+            gen = argparse.Namespace(**{**vars(args), "effmap_source": "generated"})
+            recon.efficiency_map(model, effmap_source(gen, wl, 16_000_000, 78, dev), *args_e)
+            torch.cuda.synchronize()
+            e0.record()
+            recon.efficiency_map(model, effmap_source(gen, wl, wl.n_effmap, 77, dev), *args_e)
+            e1.record()
+            torch.cuda.synchronize()
+            effmap["generated_ms"] = max_over_ranks(e0.elapsed_time(e1), world)
         if wl.name == "tor_tof_128x128x64_10M" and world == 1:
             osem = time_osem(model, data, effinv, wl, dev)
 

@@ -118,10 +118,13 @@ int srf_tor_backproject_adjoint(const float *x1, const float *y1, const float *z
  * of dominant-axis group `axis` (0 x, 1 y, 2 z) are mapped with lors_value = 1 into
  * `image`, in that group's kernel layout (grid / center / size as for srf_tor_maplors).
  * Every kernel of the call makes LOR t again from its number:
- *   kind 0: a uniform pair of distinct crystals: a = floor(u1 n / 2^32),
- *           b = floor(u2 (n - 1) / 2^32) shifted up past a, (u1, u2) the high and low
- *           halves of SplitMix64 output first + t of the stream seeded `seed`, n the
- *           crystal count;
+ *   kind 0: a random chord of a ring scanner (n_rings rings of n_per_block crystals,
+ *           crystal k of ring r at index r * n_per_block + k, angle 2 pi k / n_per_block;
+ *           n_blocks = 1): groups of 256 consecutive numbers share the chord class
+ *           s = (k_a + k_b) mod n and the ring offset r_b - r_a, drawn from SplitMix64
+ *           outputs 4 group and 4 group + 2 of the stream seeded `seed`; k_a and r_a come
+ *           from output 2 g + 1 (g = first + t). Every ordered crystal pair is equally
+ *           likely; a crystal paired with itself maps nothing;
  *   kind 1: the scanner's block-pair enumeration in the reference's order (ring pairs
  *           ir1-major, srfapp_new.py:153-157; block pairs i1 < i2 in a ring, i1 != i2
  *           across rings, scanner/pet/pet.py:149-168; every crystal of the first block,

@@ -22,6 +22,16 @@ __device__ __forceinline__ float pick(const float *a, int k) {
     return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]);
 }
 
+// The dominant axis of an event (dominentBy, :70-77): 0 x, 1 y, 2 z, -1 none (NaN).
+__device__ __forceinline__ int dominant_axis(const float *e) {
+    const float ax = fabsf(__fsub_rn(e[3], e[0])), ay = fabsf(__fsub_rn(e[4], e[1]));
+    const float az = fabsf(__fsub_rn(e[5], e[2]));
+    if (ax >= ay && ax >= az) return 0;
+    if (ay > ax && ay >= az) return 1;
+    if (az > ax && az > ay) return 2;
+    return -1;
+}
+
 // One event -> its bucket and output record. RECON selects recon_process (10
 // columns out) vs map_process (7 columns out).
 template <bool RECON>
@@ -37,12 +47,7 @@ __device__ __forceinline__ Rec process(const float *e, bool cut, float limit) {
     const float rsq = __fadd_rn(__fadd_rn(__fadd_rn(sq(x1), sq(x2)), sq(y1)), sq(y2));
     const float f = __fdiv_rn(__fdiv_rn(__fdiv_rn(sq(dsq), rsq), p_dis2), 2.0f);
     // dominant axis (dominentBy)
-    const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
-    int axis;
-    if (ax >= ay && ax >= az) axis = 0;
-    else if (ay > ax && ay >= az) axis = 1;
-    else if (az > ax && az > ay) axis = 2;
-    else axis = -1;
+    const int axis = dominant_axis(e);
     if (axis < 0) {
         r.bucket = kBuckets;
         return r;

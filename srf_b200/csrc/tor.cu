@@ -93,22 +93,51 @@ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long s,
     return z ^ (z >> 31);
 }
 
-// Crystal indices (a, b) of LOR number g.
-//   gen 1: a = floor(u1 n / 2^32), b = floor(u2 (n - 1) / 2^32) shifted up past a, with
-//          (u1, u2) the high and low halves of splitmix64(seed, g) and n the crystal count;
+// Crystal indices (a, b) of LOR number g; false for a pair of one crystal with itself.
+//   gen 1: random chords of a ring scanner (crystal a_pos of ring r at index
+//          r * n_per_block + a_pos, angle 2 pi a_pos / n_per_block). LORs come in groups of
+//          kChordGroup consecutive numbers that share the transverse direction (the chord
+//          class s = a_pos + b_pos mod n) and the ring offset d = r_b - r_a: with
+//          (h1, l1) the high and low halves of splitmix64(seed, 4 group) and h2 the high
+//          half of splitmix64(seed, 4 group + 2), s = floor(h1 n / 2^32) and d = j2 - j1,
+//          j1 = floor(l1 nr / 2^32), j2 = floor(h2 nr / 2^32); per LOR, with (h, l) the
+//          halves of splitmix64(seed, 2 g + 1) and i = g mod kChordGroup, a_pos =
+//          floor(n (i + h / 2^32) / kChordGroup) (stratified: a uniform position, LOR i of a
+//          group in the i-th part of the ring), b_pos = s - a_pos mod n and r_a =
+//          max(0, -d) + floor(l (nr - |d|) / 2^32). Every ordered pair of
+//          crystals is equally likely (s and a_pos uniform; d distributed as the
+//          difference of two uniform rings, r_a uniform given d), and a warp's LORs
+//          share a direction, so the slab kernels walk fewer wasted voxel slots than for
+//          pairs drawn one by one;
 //   gen 2: the g-th pair of the reference's effmap enumeration (srfapp_new.py:153-157 over
 //          scanner/pet/pet.py:149-177): ring pairs (ir1, ir2) ir1-major, in each the block
 //          pairs i1 < i2 (same ring) or i1 != i2 (different rings) row-major, in each every
 //          crystal of the first block (major) with every crystal of the second.
-__device__ __forceinline__ void gen_pair(const TorParams &p, long long g, int &a, int &b) {
+constexpr long long kChordGroup = 256;
+
+__device__ __forceinline__ unsigned scale32(unsigned u, unsigned n) {
+    return (unsigned)(((unsigned long long)u * n) >> 32);
+}
+
+__device__ __forceinline__ bool gen_pair(const TorParams &p, long long g, int &a, int &b) {
     if (p.gen == 1) {
-        const unsigned n = (unsigned)(p.n_rings * p.n_blocks * p.n_per_block);
-        const unsigned long long h = splitmix64(p.gen_seed, (unsigned long long)g);
-        const unsigned u1 = (unsigned)(h >> 32), u2 = (unsigned)h;
-        a = (int)(((unsigned long long)u1 * n) >> 32);
-        const int j = (int)(((unsigned long long)u2 * (n - 1u)) >> 32);
-        b = j + (j >= a ? 1 : 0);
-        return;
+        const unsigned n = (unsigned)p.n_per_block, nr = (unsigned)p.n_rings;
+        const unsigned long long grp = (unsigned long long)(g / kChordGroup);
+        const unsigned long long hg = splitmix64(p.gen_seed, 4ull * grp);
+        const unsigned long long hg2 = splitmix64(p.gen_seed, 4ull * grp + 2ull);
+        const unsigned s = scale32((unsigned)(hg >> 32), n);
+        const int d = (int)scale32((unsigned)(hg2 >> 32), nr) - (int)scale32((unsigned)hg, nr);
+        const unsigned long long h = splitmix64(p.gen_seed, 2ull * (unsigned long long)g + 1ull);
+        // stratified over the group: LOR i of the group draws a_pos in the i-th of
+        // kChordGroup equal parts of the ring, so neighbours are near-identical chords
+        const unsigned long long i = (unsigned long long)(g % kChordGroup);
+        const unsigned a_pos = (unsigned)((((i << 32) | (h >> 32)) * n) >> 40);
+        const unsigned b_pos = (s + n - a_pos) % n;
+        const int r_lo = max(0, -d);
+        const int r_a = r_lo + (int)scale32((unsigned)h, nr - (unsigned)abs(d));
+        a = r_a * (int)n + (int)a_pos;
+        b = (r_a + d) * (int)n + (int)b_pos;
+        return a != b;
     }
     const long long nb = p.n_blocks, cb = (long long)p.n_per_block * p.n_per_block;
     const long long n_same = nb * (nb - 1) / 2 * cb, n_cross = nb * (nb - 1) * cb;
@@ -147,19 +176,22 @@ __device__ __forceinline__ void gen_pair(const TorParams &p, long long g, int &a
     const long long c1 = rc / p.n_per_block, c2 = rc - c1 * p.n_per_block;
     a = (int)((ir1 * nb + i1) * p.n_per_block + c1);
     b = (int)((ir2 * nb + i2) * p.n_per_block + c2);
+    return true;
 }
 
 // The map record columns of generated LOR t (x1, y1, z1, x2, y2, z2, f after
 // map_process's swap and permutation); false when its dominant axis is another group's.
 __device__ __forceinline__ bool gen_columns(const TorParams &p, int64_t t, float (&c)[7]) {
     int a, b;
-    gen_pair(p, (long long)(p.gen_first + t), a, b);
+    if (!gen_pair(p, (long long)(p.gen_first + t), a, b)) return false;
     float e[6];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         e[k] = __ldg(p.crystals + 3 * (int64_t)a + k);
         e[3 + k] = __ldg(p.crystals + 3 * (int64_t)b + k);
     }
+    // the dominant axis first (process's own test): another group's LOR costs no more
+    if (dominant_axis(e) != p.gen_axis) return false;
     const Rec r = process<false>(e, false, 0.0f);  // map_process (on_tor_lors.py:243-248)
     if (r.bucket >= kBuckets || (r.bucket >> 1) != p.gen_axis) return false;
 #pragma unroll
@@ -176,6 +208,7 @@ __device__ __forceinline__ bool lor_columns(const TorParams &p, int64_t t, float
                                             float &f) {
     if constexpr (kGen) {
         static_assert(OP == kMap, "generated LORs are map LORs");
+        static_assert(kChordGroup == 256, "the stratified draw shifts by 40 = 32 + log2(256)");
         float c[7];
         if (!gen_columns(p, t, c)) return false;
         x1 = c[0]; y1 = c[1]; z1 = c[2]; x2 = c[3]; y2 = c[4]; z2 = c[5]; f = c[6];
@@ -821,22 +854,6 @@ struct SegPlan {
     LorRec *rec;           // [n] per-LOR records written by seg_count
 };
 
-// LOR t's constants in a slab kernel: from the record the binning wrote, or, for generated
-// map LORs (no records: nothing per LOR is kept in memory), derived again from the LOR.
-template <int OP, bool kGen>
-__device__ __forceinline__ bool slab_lor(const TorParams &p, const SegPlan &sp, int64_t t,
-                                         LorConst &L) {
-    if constexpr (kGen) return lor_prepare<OP, true>(p, t, L);
-    return lor_load<OP>(p, sp.rec, t, L);
-}
-
-template <int OP, bool kGen>
-__device__ __forceinline__ bool slab_lor_geometry(const TorParams &p, const SegPlan &sp,
-                                                  int64_t t, LorConst &L) {
-    if constexpr (kGen) return lor_geometry<OP, true>(p, t, L);
-    return lor_rec_geometry(sp.rec, t, L);
-}
-
 // Slab ids of LOR t (slice range k of its frame, row band b): id = k * nbands + b, with k
 // counted over frames. Calls g(id) for each. With row bands, the bands of slice range k
 // are those the LOR's window rows can reach in its slices there: the rows follow the
@@ -900,8 +917,8 @@ __global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams 
         if (t >= p.n) break;
         int packed = -1;
         LorConst L;
-        bool ok = geometry_any<OP>(p, t, L);
-        if (sp.rec) {
+        bool ok = geometry_any<OP>(p, t, L);  // generated map LORs are made here
+        if (ok) {  // only LORs that enter the slab lists are ever read back
             const LorRec r = make_rec(L, ok);
             float4 *q = reinterpret_cast<float4 *>(sp.rec + t);
             q[0] = r.a;
@@ -986,7 +1003,7 @@ __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p
         const int k_lo = packed & 0xffff, k_hi = packed >> 16;
         int s_lo = 0, s_hi = p.gz - 1;
         float y1 = 0.f, z1 = 0.f, d1 = 0.f, dz = 1.f;
-        if (kBand && sp.rec) {  // the values seg_count used, from the LOR's record
+        if (kBand) {  // the values seg_count used, from the LOR's record
             const float4 *q = reinterpret_cast<const float4 *>(sp.rec + t);
             const float4 a = q[0], b = q[1], d = q[3];
             const int sl = __float_as_int(d.w);
@@ -996,15 +1013,6 @@ __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p
             z1 = a.z;
             d1 = b.x;
             dz = b.y;
-        } else if (kBand) {  // generated map LORs: the same values, derived again
-            LorConst L;
-            lor_geometry<kMap, true>(p, t, L);
-            s_lo = L.s_lo;
-            s_hi = L.s_hi;
-            y1 = L.y1;
-            z1 = L.z1;
-            d1 = L.d1;
-            dz = L.dz;
         }
         lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi, y1, z1, d1, dz, [&](int id) {
             const int pos = warp_increment(cursor, id);
@@ -1041,7 +1049,7 @@ __host__ __device__ __forceinline__ int slab_floats(int nsl, int gx, int gy, int
 // at a time (one item per lane, the LOR's constants read from its record); otherwise
 // each lane walks its own segment's slices.
 // kBand: the slabs are bands of rows (sp.nbands > 1), so rows are limited to the band.
-template <int OP, int P, bool kExpand, bool kBand, bool kGen = false>
+template <int OP, int P, bool kExpand, bool kBand>
 __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorParams p, SegPlan sp) {
     extern __shared__ float slab[];
     __shared__ signed char owner_tab[kSlabThreads / 32][32];
@@ -1102,7 +1110,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
             int a = 0, cnt = 0, t = -1;
             if (q < end) {
                 t = sp.seg[q];
-                if (slab_lor<OP, kGen>(p, sp, t, L)) {
+                if (lor_load<OP>(p, sp.rec, t, L)) {
                     a = max(L.s_lo, S0);
                     cnt = max(0, min(L.s_hi, S1 - 1) - a + 1);
                 }
@@ -1155,7 +1163,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
                 const float k0s_o = __shfl_sync(0xffffffffu, L.k0s, o);
                 const bool all_o = OP == kMap && __shfl_sync(0xffffffffu, (int)L.all, o);
                 if (valid) {
-                    slab_lor_geometry<OP, kGen>(p, sp, t_o, M);
+                    lor_rec_geometry(sp.rec, t_o, M);
                     M.scale = scale_o;
                     M.k0s = k0s_o;
                     M.all = all_o;
@@ -1356,17 +1364,8 @@ int slab_kernel(const TorParams &p, bool band, void (**kern)(const TorParams, Se
     *kern = p.slab_expand
                 ? (band ? tor_slab_kernel<OP, P, true, true> : tor_slab_kernel<OP, P, true, false>)
                 : (band ? tor_slab_kernel<OP, P, false, true> : tor_slab_kernel<OP, P, false, false>);
-    int which = (p.slab_expand ? 2 : 0) + (band ? 1 : 0);
-    if constexpr (OP == kMap) {
-        // generated LORs: their own instances, so the others carry no generator code
-        if (p.gen) {
-            *kern = band ? tor_slab_kernel<OP, P, false, true, true>
-                         : tor_slab_kernel<OP, P, false, false, true>;
-            which = 4 + (band ? 1 : 0);
-        }
-    }
-    static std::atomic<unsigned long long> attr_set[6];  // per kernel instance, per device
-    std::atomic<unsigned long long> &done = attr_set[which];
+    static std::atomic<unsigned long long> attr_set[4];  // per kernel instance, per device
+    std::atomic<unsigned long long> &done = attr_set[(p.slab_expand ? 2 : 0) + (band ? 1 : 0)];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
     if (!(done.load() & (1ull << dev))) {
@@ -1395,7 +1394,7 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
     const int64_t max_slabs_per_lor = (int64_t)sp.slabs_pf * sp.nbands;
     const size_t budget = (size_t)g_seg_scratch_bytes.load(std::memory_order_relaxed);
     int64_t chunk = (int64_t)(budget / (sizeof(int) * (size_t)max_slabs_per_lor +
-                                        (p.gen ? 0 : sizeof(LorRec)) + sizeof(int)));
+                                        sizeof(LorRec) + sizeof(int)));
     chunk = std::max<int64_t>(kSegTile, chunk / kSegTile * kSegTile);
     chunk = std::min<int64_t>(chunk, p.n);
     sp.ntiles = (int)((chunk + kSegTile - 1) / kSegTile);
@@ -1407,7 +1406,7 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
     const size_t b_offs = al(sizeof(int64_t) * (size_t)sp.ntiles * sp.n_slabs);
     const size_t b_slab = al(sizeof(int64_t) * (2 * sp.n_slabs + 1));
     const size_t b_seg = al(sizeof(int) * cap);
-    const size_t b_rec = p.gen ? 0 : al(sizeof(LorRec) * chunk);  // generated: none
+    const size_t b_rec = al(sizeof(LorRec) * chunk);
     char *ws = nullptr;
     cudaError_t e = scratch_alloc((void **)&ws,
                                   b_rec + b_range + b_counts + b_offs + b_slab + b_seg, stream);
@@ -1415,7 +1414,7 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
         set_cuda_error(e);
         return SRF_ERR_CUDA;
     }
-    sp.rec = p.gen ? nullptr : reinterpret_cast<LorRec *>(ws);
+    sp.rec = reinterpret_cast<LorRec *>(ws);
     char *w2 = ws + b_rec;
     sp.range = reinterpret_cast<int *>(w2);
     sp.tile_counts = reinterpret_cast<int *>(w2 + b_range);
@@ -1671,6 +1670,7 @@ extern "C" int srf_tor_maplors_generated(int kind, const float *crystals, int n_
     if (n_rings < 1 || n_blocks < 1 || n_per_block < 1) return SRF_ERR_INVALID_ARGUMENT;
     const int64_t n_cry = (int64_t)n_rings * n_blocks * n_per_block;
     if (n_cry < 2 || n_cry > ((int64_t)1 << 31) - 1) return SRF_ERR_INVALID_ARGUMENT;
+    if (kind == 0 && n_blocks != 1) return SRF_ERR_INVALID_ARGUMENT;  // rings of crystals
     if (kind == 1) {
         if (n_blocks < 2) return SRF_ERR_INVALID_ARGUMENT;
         const double cb = (double)n_per_block * n_per_block;

@@ -226,24 +226,45 @@ def splitmix64(seed, k):
         return z ^ (z >> np.uint64(31))
 
 
-def random_pair_indices(n_crystals, seed, first, count):
-    """Crystal indices (a, b) of generated random pairs first .. first+count-1: the host
-    mirror of kind 0 of ``srf_tor_maplors_generated`` (a = floor(u1 n / 2^32), b =
-    floor(u2 (n - 1) / 2^32) shifted up past a, (u1, u2) the halves of SplitMix64)."""
-    h = splitmix64(seed, np.arange(first, first + count, dtype=np.uint64))
-    u1, u2 = h >> np.uint64(32), h & np.uint64(0xFFFFFFFF)
-    n = np.uint64(n_crystals)
-    a = ((u1 * n) >> np.uint64(32)).astype(np.int64)
-    j = ((u2 * (n - np.uint64(1))) >> np.uint64(32)).astype(np.int64)
-    return a, j + (j >= a)
+CHORD_GROUP = 256
+
+
+def random_pair_indices(n_rings, n_per_ring, seed, first, count):
+    """Crystal indices (a, b) of generated random chords first .. first+count-1 of a ring
+    scanner (crystal k of ring r at index r * n_per_ring + k): the host mirror of kind 0
+    of ``srf_tor_maplors_generated``. Groups of ``CHORD_GROUP`` consecutive numbers share
+    the chord class s = (k_a + k_b) mod n (the transverse direction) and the ring offset
+    d = r_b - r_a; within a group r_a is drawn per LOR and k_a stratified (LOR i of a
+    group in the i-th of CHORD_GROUP equal parts of the ring), so neighbouring LORs are
+    near-identical chords. Every ordered crystal pair is equally likely; a pair of one
+    crystal with itself (a == b) maps nothing."""
+    n, nr = np.uint64(n_per_ring), np.uint64(n_rings)
+    g = np.arange(first, first + count, dtype=np.uint64)
+    grp = g // np.uint64(CHORD_GROUP)
+    hg = splitmix64(seed, np.uint64(4) * grp)
+    hg2 = splitmix64(seed, np.uint64(4) * grp + np.uint64(2))
+    hi, lo = np.uint64(32), np.uint64(0xFFFFFFFF)
+
+    def scale(u, m):
+        return ((u * m) >> hi).astype(np.int64)
+
+    s = scale(hg >> hi, n)
+    d = scale(hg2 >> hi, nr) - scale(hg & lo, nr)
+    h = splitmix64(seed, np.uint64(2) * g + np.uint64(1))
+    i = g % np.uint64(CHORD_GROUP)  # stratified: LOR i of a group in the i-th part of the ring
+    a_pos = ((((i << hi) | (h >> hi)) * n) >> np.uint64(40)).astype(np.int64)
+    b_pos = (s + int(n) - a_pos) % int(n)
+    r_a = np.maximum(0, -d) + scale(h & lo, (np.int64(n_rings) - np.abs(d)).astype(np.uint64))
+    return r_a * int(n) + a_pos, (r_a + d) * int(n) + b_pos
 
 
 class GeneratedPairs:
     """Detector-pair LORs that the TOR map kernels make on the fly from their number, so
     that no LOR array exists at any point (``srf_tor_maplors_generated``):
 
-    * ``GeneratedPairs.random(scanner, n, seed)``: n uniform pairs of distinct crystals
-      (SplitMix64, see ``random_pair_indices``);
+    * ``GeneratedPairs.random(scanner, n, seed)``: n uniform crystal pairs of a ring
+      scanner, drawn in groups that share a direction (SplitMix64, see
+      ``random_pair_indices``);
     * ``GeneratedPairs.block_pairs(cylindrical_pet)``: every crystal pair of the scanner's
       block pairs over all ring pairs, in the reference's effmap order
       (srfapp_new.py:153-157, scanner/pet/pet.py:149-177).
@@ -267,8 +288,9 @@ class GeneratedPairs:
 
     @classmethod
     def random(cls, scanner, n, seed, chunk=1 << 26, device="cuda"):
+        """n random chords of a ``RingScanner`` (``random_pair_indices``)."""
         pos = scanner.crystal_positions()
-        return cls(0, pos, n, seed, 1, 1, len(pos), chunk, device)
+        return cls(0, pos, n, seed, scanner.n_rings, 1, scanner.n_crystals, chunk, device)
 
     @classmethod
     def block_pairs(cls, pet, chunk=1 << 26, device="cuda"):
@@ -285,7 +307,7 @@ class GeneratedPairs:
     def pair_indices(self, first, count):
         """(a, b) crystal indices of LORs first .. first+count-1 (host)."""
         if self.kind == 0:
-            return random_pair_indices(len(self.host_crystals), self.seed, first, count)
+            return random_pair_indices(self.n_rings, self.n_per_block, self.seed, first, count)
         nr, nb, ncb = self.n_rings, self.n_blocks, self.n_per_block
         a_all, b_all = [], []
         for ir1 in range(nr):
@@ -301,6 +323,8 @@ class GeneratedPairs:
         return a[first:first + count], b[first:first + count]
 
     def host_lors(self, first, count):
+        """The same LORs as the kernels make, [count, 6] (a pair of one crystal with itself,
+        which the kernels skip, comes out with both ends equal)."""
         a, b = self.pair_indices(first, count)
         return np.hstack([self.host_crystals[a], self.host_crystals[b]])
 

@@ -38,14 +38,25 @@ def test_splitmix64_matches_the_published_stream():
         assert got == _splitmix64_stream(seed, 64)
 
 
-def test_random_pairs_distinct_and_in_range():
-    a, b = random_pair_indices(1000, 9, 123, 200_000)
-    assert a.min() >= 0 and b.min() >= 0 and a.max() < 1000 and b.max() < 1000
-    assert not np.any(a == b)
+def test_random_chords_in_range_uniform_and_grouped():
+    nr, nc = 8, 50
+    a, b = random_pair_indices(nr, nc, 9, 123, 400_000)
+    assert a.min() >= 0 and b.min() >= 0 and a.max() < nr * nc and b.max() < nr * nc
     # chunks are independent of where a call starts
-    a2, b2 = random_pair_indices(1000, 9, 123 + 5000, 10)
+    a2, b2 = random_pair_indices(nr, nc, 9, 123 + 5000, 10)
     np.testing.assert_array_equal(a[5000:5010], a2)
     np.testing.assert_array_equal(b[5000:5010], b2)
+    # every ordered pair equally likely: ring pairs and in-ring positions each uniform
+    ra, rb, ka, kb = a // nc, b // nc, a % nc, b % nc
+    h = np.bincount(ra * nr + rb, minlength=nr * nr)
+    assert abs(h.std() / h.mean()) < 0.08
+    hk = np.bincount(ka * nc + kb, minlength=nc * nc)
+    assert abs(hk.std() / hk.mean()) < 0.25
+    # a group of 256 numbers shares its chord class and ring offset
+    g0 = (123 // 256 + 1) * 256 - 123
+    grp = slice(g0, g0 + 256)
+    assert len(np.unique((ka[grp] + kb[grp]) % nc)) == 1
+    assert len(np.unique(rb[grp] - ra[grp])) == 1
 
 
 def test_block_pair_enumeration_matches_the_scanner():
