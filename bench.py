@@ -706,11 +706,13 @@ def run_siddon(args):
     timer = profiling.KernelTimer()
     launches0 = _lib.call_raw("srf_launch_count")
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("bench_timed")
     with timer:
         start.record()
         for _ in range(args.steps):
             step()
         end.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier(world)
     gpu_launches = _lib.call_raw("srf_launch_count") - launches0
