@@ -59,6 +59,18 @@ METRICS = {
 UNIT = "LORs/s"
 
 
+# When set to a list, bench lines are collected there instead of printed (the default run
+# embeds the other workloads' lines in its own).
+_COLLECT = None
+
+
+def emit(line):
+    if _COLLECT is not None:
+        _COLLECT.append(line)
+    else:
+        print(json.dumps(line), flush=True)
+
+
 def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -99,6 +111,10 @@ def parse_args(argv=None):
                          "ordered by direction (tensor, the default: the faster path), or "
                          "made inside the map kernels from their number with no LOR array "
                          "(generated)")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="default workload: skip the runs of the other configurations "
+                         "(Siddon 64, batched 96, differentiable 128, large FOV 256) whose "
+                         "summaries the line carries under 'configs'")
     ap.add_argument("--tuning", default=None,
                     help="PATH,SLAB_SLICES,GRID_MULT for srf_tor_set_tuning, or PATH for "
                          "srf_siddon_set_tuning with --workload siddon64 (default: the "
@@ -266,7 +282,7 @@ def run_large_recon(args):
                     "on-device random pairs -> map_process -> maplors; OSEM: subsets split "
                     "and ordered once, then per subset one combined projection + "
                     "back-projection call per axis group and the update"}
-    print(json.dumps(line), flush=True)
+    emit(line)
     return 0
 
 
@@ -790,7 +806,7 @@ def run_siddon(args):
                          "effmap_lors": 10_000_000},
                 "roofline": roof, "cpu_baseline": base, "e2e": e2e,
                 "gpu_launches": gpu_launches, "clocks": clk}
-        print(json.dumps(line), flush=True)
+        emit(line)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -896,7 +912,7 @@ def run_autograd(args):
             "data": "synthetic (seeded per-frame phantoms)",
             "config": {"workload": "autograd_128x128x64_8x5M", "grid": list(wl.grid),
                        "voxel_mm": wl.voxel, "checkpoint": True, "beta": 0.01}}
-    print(json.dumps(line), flush=True)
+    emit(line)
     return 0
 
 
@@ -967,7 +983,7 @@ def run_reference(args):
                                        f"preprocessed events"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    emit(line)
     return 0
 
 
@@ -1061,8 +1077,51 @@ def run_batched(args):
             "config": {"workload": "batched_96x96x48_64frames", "grid": grid,
                        "voxel_mm": wl0.voxel, "kernel_width": round(wl0.kernel_width, 4),
                        "tof_res_ps": wl0.tof_res_ps, "subsets": S_sub}}
-    print(json.dumps(line), flush=True)
+    emit(line)
     return 0
+
+
+def _pick(d, *keys):
+    out = {}
+    for k in keys:
+        v = d
+        for part in k.split("."):
+            v = v.get(part) if isinstance(v, dict) else None
+        out[k.replace(".", "_")] = v
+    return out
+
+
+def run_other_configs():
+    """The other BASELINE configurations, each run in this process after the default
+    step's measurement, summarised (their full lines come from ``--workload NAME``)."""
+    global _COLLECT
+    plan = [
+        ("config1_siddon64", ["--workload", "siddon64"],
+         ("metric", "value", "unit", "ms_per_step", "e2e.value", "osem_iteration_ms",
+          "roofline.bound", "roofline.frac", "cpu_baseline.value", "clocks.sm_mhz")),
+        ("config3_batched96", ["--workload", "batched96"],
+         ("metric", "value", "unit", "plain_loop_ms", "speedup_vs_plain",
+          "rel_l2_batched_vs_plain_max", "autotuned")),
+        ("config4_autograd128", ["--workload", "autograd128"],
+         ("metric", "value", "unit", "adjoint_identity_rel_err", "frames", "events_per_frame",
+          "gradient_finite")),
+        ("config5_large256", ["--workload", "large256", "--no-variants", "--cpu-seconds", "4"],
+         ("metric", "value", "unit", "ms_per_step", "e2e.value", "roofline.bound",
+          "roofline.frac", "effmap.ms", "effmap.lors", "effmap.generated_ms",
+          "cpu_baseline.value")),
+    ]
+    out = {}
+    for name, argv, keys in plan:
+        _COLLECT = []
+        try:
+            main(argv + ["--no-configs"])
+            out[name] = _pick(_COLLECT[-1], *keys) if _COLLECT else {"error": "no line"}
+        except Exception as exc:  # one configuration failing does not hide the others
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"}
+        finally:
+            _COLLECT = None
+            torch.cuda.empty_cache()
+    return out
 
 
 def main(argv=None):
@@ -1248,7 +1307,9 @@ def main(argv=None):
                 "roofline": roof, "cpu_baseline": base, "e2e": e2e,
                 "gpu_launches": gpu_launches, "clocks": clk, "variants": variants,
                 "effmap": effmap, "osem": osem}
-        print(json.dumps(line), flush=True)
+        if args.configs and world == 1 and args.workload == "tor128":
+            line["configs"] = run_other_configs()
+        emit(line)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
