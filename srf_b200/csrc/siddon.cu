@@ -11,10 +11,9 @@
 // and copies the geometry device-to-host first). The walk state (next boundary,
 // step, voxel counters) is evaluated with the same float operations as the reference,
 // so each ray visits the same voxels with the same chord lengths; the TOF weight of a
-// voxel uses float arithmetic for the Gaussian itself. The image is read and reduced
-// into four consecutive voxels at a time where a ray's run allows (siddon_kernel).
+// voxel uses float arithmetic for the Gaussian itself. The scatter ops reduce into four
+// consecutive voxels at a time where a ray's run allows (siddon_kernel).
 
-#include <algorithm>
 #include <atomic>
 #include <cfloat>
 #include <cmath>
@@ -166,11 +165,11 @@ __device__ __forceinline__ bool ray_setup(const SiddonParams &p, int64_t t, Ray 
 }
 
 // Adds four consecutive floats with one reduction (16-byte aligned address). Like a scalar
-// float atomic add, it flushes subnormal inputs and results to zero.
+// float atomic add, it flushes subnormal inputs and results to zero. No memory clobber: the
+// kernels that issue it never read the image they reduce into.
 __device__ __forceinline__ void red_quad(float *q, float a, float b, float c, float d) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};"
-                 :: "l"(q), "f"(a), "f"(b), "f"(c), "f"(d)
-                 : "memory");
+                 :: "l"(q), "f"(a), "f"(b), "f"(c), "f"(d));
 }
 
 // One thread per ray: RayTracing / BackRayTracing / Map (siddon.cu.cc:293-415) and the
@@ -199,6 +198,7 @@ __global__ void __launch_bounds__(256) siddon_kernel(const SiddonParams p) {
         float acc = 0.0f;
         int n_visits = 0;
         if (ray_setup<OP>(p, t, R)) {
+            float pend_v = 0.0f, pend_w = 0.0f;           // projection: the last gather
             int cur = -1;                                  // kQuad: current quad (index / 4)
             float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);  // its values or pending adds
             float last_t = 0.0f;
@@ -225,10 +225,15 @@ __global__ void __launch_bounds__(256) siddon_kernel(const SiddonParams p) {
                 const int mi = R.boffs;
                 if (OP != kCount && use) {
                     if (!kQuad) {
-                        if (OP == kProj)
-                            acc = fmaf(__ldg(p.image_in + mi), val, acc);
-                        else
+                        if (OP == kProj) {
+                            // the gather is consumed one voxel later, so its latency
+                            // overlaps the next step of the walk; same sum, same order
+                            acc = fmaf(pend_v, pend_w, acc);
+                            pend_v = __ldg(p.image_in + mi);
+                            pend_w = val;
+                        } else {
                             atomicAdd(p.image_out + mi, val * R.oscale);
+                        }
                     } else {
                         const int qd = mi >> 2, r = mi & 3;
                         if (qd != cur) {
@@ -257,6 +262,7 @@ __global__ void __launch_bounds__(256) siddon_kernel(const SiddonParams p) {
             }
             if (kQuad && OP != kProj && OP != kCount && cur >= 0)
                 red_quad(p.image_out + 4 * (int64_t)cur, qv.x, qv.y, qv.z, qv.w);
+            if (OP == kProj) acc = fmaf(pend_v, pend_w, acc);
         }
         if (OP == kProj) p.proj_out[t] = acc;
         if (OP == kCount) p.count_out[t] = n_visits;
