@@ -57,3 +57,28 @@ def test_invalid_arguments_rejected_before_any_launch():
     assert st == 1
     assert lib.srf_preprocess_workspace_size(-1) == -1
     assert lib.srf_preprocess_workspace_size(10) > 0
+
+
+def test_new_entry_points_validate_before_any_launch():
+    """The fused PSF, the generated-LOR map and the Siddon family switch reject bad
+    arguments on the host (status 1 invalid argument, 3 unsupported) without a GPU."""
+    lib = _lib.load()
+    unsupported = 3
+    # PSF: nz above the shared-memory limit, a bad orientation flag, a negative size
+    assert lib.srf_psf_apply(None, None, None, 4, 4, None, 300, None, 0, None, 0, None) \
+        == unsupported
+    assert lib.srf_psf_apply(None, None, None, 4, 4, None, 8, None, 2, None, 0, None) == 1
+    assert lib.srf_psf_apply(None, None, None, -1, 4, None, 8, None, 0, None, 0, None) == 1
+    # generated map LORs: unknown kind, bad axis, a ring scanner given blocks, a block-pair
+    # range past the enumeration's end
+    g = (ctypes.c_int * 3)(4, 4, 4)
+    c = (ctypes.c_float * 3)(0, 0, 0)
+    s = (ctypes.c_float * 3)(1, 1, 1)
+    f = lib.srf_tor_maplors_generated
+    assert f(2, None, 1, 1, 8, 0, 0, 10, 0, 0, g, c, s, 1.0, None, 0, None) == 1
+    assert f(0, None, 1, 1, 8, 0, 0, 10, 3, 0, g, c, s, 1.0, None, 0, None) == 1
+    assert f(0, None, 2, 3, 8, 0, 0, 10, 0, 0, g, c, s, 1.0, None, 0, None) == 1
+    # 2 rings x 2 blocks x 1 crystal: 2 * (1 * 2 + 1) = 6 pairs
+    assert f(1, None, 2, 2, 1, 0, 5, 2, 0, 0, g, c, s, 1.0, None, 0, None) == 1
+    assert lib.srf_siddon_set_tuning(2) == 1
+    assert lib.srf_siddon_set_tuning(0) == 0
