@@ -846,6 +846,7 @@ struct SegPlan {
     int nsl, n_slabs, ntiles;  // n_slabs counts slab ids over all frames
     int slabs_pf;              // slice ranges per frame
     int nbands, band_rows;     // row bands per slice range and rows per band (last: fewer)
+    unsigned band_magic;       // ceil(2^32 / band_rows): r / band_rows = umulhi(r, magic)
     int *range;            // [n] packed k_lo | k_hi << 16, or -1
     int *tile_counts;      // [ntiles * n_slabs]
     int64_t *tile_offs;    // [ntiles * n_slabs]
@@ -869,8 +870,14 @@ __device__ __forceinline__ void lor_slab_ids(const TorParams &p, const SegPlan &
         return;
     }
     const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
+    // the crossing's position along the LOR at slice s, r(s) = (z_s - z1) / dz, as
+    // r0 + s * rs: within a few ulps of the division, far inside the two rows of margin
+    // (the division itself where 1 / dz would overflow)
+    const bool lin = fabsf(dz) > 1.0e-30f;
+    const float inv_dz = lin ? 1.0f / dz : 0.0f;
+    const float r0 = (p.slice0_f - z1) * inv_dz, rs = p.inter_z * inv_dz;
     auto y_at = [&](int s) {
-        const float r = (p.slice0_f + (float)s * p.inter_z - z1) / dz;
+        const float r = lin ? fmaf((float)s, rs, r0) : (p.slice0_f + (float)s * p.inter_z - z1) / dz;
         return fmaf(d1, fminf(fmaxf(r, 0.0f), 1.0f), y1);
     };
     for (int k = k_lo; k <= k_hi; k++) {
@@ -884,8 +891,9 @@ __device__ __forceinline__ void lor_slab_ids(const TorParams &p, const SegPlan &
             const int r_lo = max((int)flo - p.half - 2, 0);
             const int r_hi = min((int)fhi - p.half + p.patch + 1, p.gy - 1);
             if (r_lo > r_hi) continue;
-            b_lo = r_lo / sp.band_rows;
-            b_hi = min(r_hi / sp.band_rows, sp.nbands - 1);
+            // 0 <= r < 2^14 and band_rows < 2^14: the multiply-high quotient is exact
+            b_lo = (int)__umulhi((unsigned)r_lo, sp.band_magic);
+            b_hi = min((int)__umulhi((unsigned)r_hi, sp.band_magic), sp.nbands - 1);
         }
         for (int b = b_lo; b <= b_hi; b++) g(k * sp.nbands + b);
     }
@@ -991,8 +999,12 @@ __global__ void seg_offsets_kernel(SegPlan sp, const int64_t *slab_tot) {
 
 template <bool kBand>
 __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p, SegPlan sp) {
-    extern __shared__ int cursor[];  // [n_slabs]
-    for (int k = threadIdx.x; k < sp.n_slabs; k += kSegThreads) cursor[k] = 0;
+    extern __shared__ int64_t tile_base[];  // [n_slabs] where this tile's run of each slab starts
+    int *cursor = reinterpret_cast<int *>(tile_base + sp.n_slabs);  // [n_slabs]
+    for (int k = threadIdx.x; k < sp.n_slabs; k += kSegThreads) {
+        cursor[k] = 0;
+        tile_base[k] = sp.slab_offs[k] + sp.tile_offs[(int64_t)blockIdx.x * sp.n_slabs + k];
+    }
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kSegTile;
     for (int it = 0; it < kSegItems; it++) {
@@ -1016,8 +1028,7 @@ __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p
         }
         lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi, y1, z1, d1, dz, [&](int id) {
             const int pos = warp_increment(cursor, id);
-            sp.seg[sp.slab_offs[id] + sp.tile_offs[(int64_t)blockIdx.x * sp.n_slabs + id] + pos] =
-                (int)t;
+            sp.seg[tile_base[id] + pos] = (int)t;
         });
     }
 }
@@ -1322,6 +1333,12 @@ bool slab_geometry(const TorParams &p, int pad, SegPlan &sp) {
         sp.nsl = n;
     }
     sp.nbands = (p.gy + sp.band_rows - 1) / sp.band_rows;
+    // floor(r / d) = (r * ceil(2^32 / d)) >> 32 for r, d < 2^14 (error term r (m d - 2^32)
+    // < 2^28 stays below 2^32); band_rows >= 2 whenever there is more than one band
+    sp.band_magic = sp.band_rows >= 2
+                        ? (unsigned)((((uint64_t)1 << 32) + (uint64_t)sp.band_rows - 1) /
+                                     (uint64_t)sp.band_rows)
+                        : 0u;
     sp.slabs_pf = (p.gz + sp.nsl - 1) / sp.nsl;
     sp.n_slabs = sp.slabs_pf * sp.nbands * std::max(1, p.n_frames);
     return sp.n_slabs <= kMaxSlabs && sp.slabs_pf * std::max(1, p.n_frames) < (1 << 16) &&
@@ -1445,6 +1462,7 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
     }
     const int mult = slab_grid_mult(OP, sp, chunk);
     const size_t hist_bytes = sizeof(int) * (size_t)sp.n_slabs;  // <= 16 KB (kMaxSlabs)
+    const size_t fill_bytes = (sizeof(int64_t) + sizeof(int)) * (size_t)sp.n_slabs;  // <= 48 KB
     for (int64_t c0 = 0; c0 < p.n && st == SRF_OK; c0 += chunk) {
         const TorParams q = lor_chunk(p, c0, std::min(chunk, p.n - c0));
         SegPlan sq = sp;
@@ -1456,9 +1474,9 @@ int launch_slab(const TorParams &p, const TorParams *p2, cudaStream_t stream) {
         seg_scan_kernel<<<sq.n_slabs, 1024, 0, stream>>>(sq, slab_tot);
         seg_offsets_kernel<<<1, 32, 0, stream>>>(sq, slab_tot);
         if (band)
-            seg_fill_kernel<true><<<sq.ntiles, kSegThreads, hist_bytes, stream>>>(q, sq);
+            seg_fill_kernel<true><<<sq.ntiles, kSegThreads, fill_bytes, stream>>>(q, sq);
         else
-            seg_fill_kernel<false><<<sq.ntiles, kSegThreads, hist_bytes, stream>>>(q, sq);
+            seg_fill_kernel<false><<<sq.ntiles, kSegThreads, fill_bytes, stream>>>(q, sq);
         kern<<<num_sms() * mult, kSlabThreads, smem, stream>>>(q, sq);
         count_launches(5);
         if constexpr (OP2 >= 0) {
