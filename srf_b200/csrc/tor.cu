@@ -855,51 +855,117 @@ struct SegPlan {
     LorRec *rec;           // [n] per-LOR records written by seg_count
 };
 
-// Slab ids of LOR t (slice range k of its frame, row band b): id = k * nbands + b, with k
-// counted over frames. Calls g(id) for each. With row bands, the bands of slice range k
-// are those the LOR's window rows can reach in its slices there: the rows follow the
-// crossing point's y, which is monotonic in the slice, so the rows of the range's two end
-// slices, with two rows of margin and the window's extent, bound them. y1, z1, d1 = y2 - y1
-// and dz = z2 - z1 come from the LOR's record, so counting and filling agree bit for bit.
-template <bool kBand, typename G>
-__device__ __forceinline__ void lor_slab_ids(const TorParams &p, const SegPlan &sp, int64_t t,
-                                             int k_lo, int k_hi, int s_lo, int s_hi, float y1,
-                                             float z1, float d1, float dz, G &&g) {
-    if constexpr (!kBand) {
-        for (int k = k_lo; k <= k_hi; k++) g(k);
-        return;
-    }
-    const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
+// Slab ids (slice range k of a LOR's frame, row band b): id = k * nbands + b, with k
+// counted over frames. With row bands, the bands of slice range k are those the LOR's
+// window rows can reach in its slices there: the rows follow the crossing point's y, which
+// is monotonic in the slice, so the rows of the range's two end slices, with two rows of
+// margin and the window's extent, bound them. y1, z1, d1 = y2 - y1 and dz = z2 - z1 come
+// from the LOR's record, so counting and filling agree bit for bit.
+struct SlabIdLor {
+    int k_lo, k_hi, s_lo, s_hi, f0;
+    float y1, d1, r0, rs, z1, dz;
+    int lin;  // y at slice s from r0 + s rs (else the division, where 1 / dz would overflow)
+};
+
+__device__ __forceinline__ SlabIdLor slab_id_lor(const TorParams &p, const SegPlan &sp,
+                                                 int64_t t, int k_lo, int k_hi, int s_lo,
+                                                 int s_hi, float y1, float z1, float d1,
+                                                 float dz) {
+    SlabIdLor c;
+    c.k_lo = k_lo;
+    c.k_hi = k_hi;
+    c.s_lo = s_lo;
+    c.s_hi = s_hi;
+    c.f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
     // the crossing's position along the LOR at slice s, r(s) = (z_s - z1) / dz, as
     // r0 + s * rs: within a few ulps of the division, far inside the two rows of margin
-    // (the division itself where 1 / dz would overflow)
-    const bool lin = fabsf(dz) > 1.0e-30f;
-    const float inv_dz = lin ? 1.0f / dz : 0.0f;
-    const float r0 = (p.slice0_f - z1) * inv_dz, rs = p.inter_z * inv_dz;
+    c.lin = fabsf(dz) > 1.0e-30f;
+    const float inv_dz = c.lin ? 1.0f / dz : 0.0f;
+    c.r0 = (p.slice0_f - z1) * inv_dz;
+    c.rs = p.inter_z * inv_dz;
+    c.y1 = y1;
+    c.d1 = d1;
+    c.z1 = z1;
+    c.dz = dz;
+    return c;
+}
+
+// LOR c's slab ids in slice range k: g(id) for each band its windows can reach.
+template <bool kBand, typename G>
+__device__ __forceinline__ void range_slab_ids(const TorParams &p, const SegPlan &sp,
+                                               const SlabIdLor &c, int k, G &&g) {
+    if constexpr (!kBand) {
+        g(k);
+        return;
+    }
     auto y_at = [&](int s) {
-        const float r = lin ? fmaf((float)s, rs, r0) : (p.slice0_f + (float)s * p.inter_z - z1) / dz;
-        return fmaf(d1, fminf(fmaxf(r, 0.0f), 1.0f), y1);
+        const float r = c.lin ? fmaf((float)s, c.rs, c.r0)
+                              : (p.slice0_f + (float)s * p.inter_z - c.z1) / c.dz;
+        return fmaf(c.d1, fminf(fmaxf(r, 0.0f), 1.0f), c.y1);
     };
-    for (int k = k_lo; k <= k_hi; k++) {
-        const int first = (k - f0) * sp.nsl;
-        const float ya = y_at(max(s_lo, first)), yb = y_at(min(s_hi, first + sp.nsl - 1));
-        const float lo = fminf(ya, yb), hi = fmaxf(ya, yb);
-        int b_lo = 0, b_hi = sp.nbands - 1;
-        if (lo == lo && hi == hi) {  // else: every band, left to the exact per-slice test
-            const float flo = fminf(fmaxf(floorf((lo - p.b_bound) * p.inv_y), -1.0e8f), 1.0e8f);
-            const float fhi = fminf(fmaxf(floorf((hi - p.b_bound) * p.inv_y), -1.0e8f), 1.0e8f);
-            const int r_lo = max((int)flo - p.half - 2, 0);
-            const int r_hi = min((int)fhi - p.half + p.patch + 1, p.gy - 1);
-            if (r_lo > r_hi) continue;
-            // 0 <= r < 2^14 and band_rows < 2^14: the multiply-high quotient is exact
-            b_lo = (int)__umulhi((unsigned)r_lo, sp.band_magic);
-            b_hi = min((int)__umulhi((unsigned)r_hi, sp.band_magic), sp.nbands - 1);
+    const int first = (k - c.f0) * sp.nsl;
+    const float ya = y_at(max(c.s_lo, first)), yb = y_at(min(c.s_hi, first + sp.nsl - 1));
+    const float lo = fminf(ya, yb), hi = fmaxf(ya, yb);
+    int b_lo = 0, b_hi = sp.nbands - 1;
+    if (lo == lo && hi == hi) {  // else: every band, left to the exact per-slice test
+        const float flo = fminf(fmaxf(floorf((lo - p.b_bound) * p.inv_y), -1.0e8f), 1.0e8f);
+        const float fhi = fminf(fmaxf(floorf((hi - p.b_bound) * p.inv_y), -1.0e8f), 1.0e8f);
+        const int r_lo = max((int)flo - p.half - 2, 0);
+        const int r_hi = min((int)fhi - p.half + p.patch + 1, p.gy - 1);
+        if (r_lo > r_hi) return;
+        // 0 <= r < 2^14 and band_rows < 2^14: the multiply-high quotient is exact
+        b_lo = (int)__umulhi((unsigned)r_lo, sp.band_magic);
+        b_hi = min((int)__umulhi((unsigned)r_hi, sp.band_magic), sp.nbands - 1);
+    }
+    for (int b = b_lo; b <= b_hi; b++) g(k * sp.nbands + b);
+}
+
+// The slab ids of the warp's LORs (lane l holds LOR t_l, `ok` when it enters the lists),
+// as (LOR, slice range) items spread over the lanes 32 at a time: g(id, t) for each. A LOR
+// meets tens of slice ranges, in numbers that differ from lane to lane, so one LOR per
+// lane would leave most lanes idle. Called by all 32 lanes of the warp.
+template <bool kBand, typename G>
+__device__ __forceinline__ void warp_slab_ids(const TorParams &p, const SegPlan &sp,
+                                              signed char (&owner)[32], bool ok, int t,
+                                              const SlabIdLor &c, G &&g) {
+    const int lane = threadIdx.x & 31;
+    const int cnt = ok ? c.k_hi - c.k_lo + 1 : 0;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int excl = incl - cnt;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    for (int base = 0; base < total; base += 32) {
+        for (int i = max(excl, base); i < min(incl, base + 32); ++i)
+            owner[i - base] = (signed char)lane;
+        __syncwarp();
+        const int item = base + lane;
+        const bool valid = item < total;
+        const int o = valid ? (int)owner[lane] : 0;
+        __syncwarp();
+        SlabIdLor m;
+        m.k_lo = __shfl_sync(0xffffffffu, c.k_lo, o);
+        const int k = m.k_lo + item - __shfl_sync(0xffffffffu, excl, o);
+        const int to = __shfl_sync(0xffffffffu, t, o);
+        if constexpr (kBand) {
+            m.s_lo = __shfl_sync(0xffffffffu, c.s_lo, o);
+            m.s_hi = __shfl_sync(0xffffffffu, c.s_hi, o);
+            m.f0 = __shfl_sync(0xffffffffu, c.f0, o);
+            m.lin = __shfl_sync(0xffffffffu, c.lin, o);
+            m.y1 = __shfl_sync(0xffffffffu, c.y1, o);
+            m.d1 = __shfl_sync(0xffffffffu, c.d1, o);
+            m.r0 = __shfl_sync(0xffffffffu, c.r0, o);
+            m.rs = __shfl_sync(0xffffffffu, c.rs, o);
+            m.z1 = __shfl_sync(0xffffffffu, c.z1, o);
+            m.dz = __shfl_sync(0xffffffffu, c.dz, o);
         }
-        for (int b = b_lo; b <= b_hi; b++) g(k * sp.nbands + b);
+        if (valid) range_slab_ids<kBand>(p, sp, m, k, [&](int id) { g(id, to); });
     }
 }
 
-// kBand: sp.nbands > 1 (slab ids over slice ranges and row bands).
 // atomicAdd(&counter[id], 1) for the calling lane, with one shared-memory update per
 // distinct id among the warp's active lanes (neighbouring LORs mostly share slabs). Returns
 // the lane's slot: the counter's old value plus its rank among the lanes with that id.
@@ -914,35 +980,54 @@ __device__ __forceinline__ int warp_increment(int *counter, int id) {
     return first + __popc(peers & ((1u << lane) - 1u));
 }
 
+// Counting. Map calls over row-band slabs spread the (LOR, slice range) items of a warp
+// over its lanes (warp_slab_ids): their LORs span the whole field of view (tens of ranges
+// each, in numbers that differ between lanes, with a band computation per range), and
+// generated LORs of another axis group drop out here, idling their lanes in a loop per
+// lane (generated random pairs at 256 x 256 x 128: 239 against 264 ms per 50M, tensor
+// pairs 217 against 220 ms). Elsewhere a loop per lane measured faster: 1.4 % on the
+// 128 x 128 x 64 combined call, 4 % on the 128 x 128 x 64 map, where a range costs one
+// shared add.
 template <int OP, bool kBand>
 __global__ void __launch_bounds__(kSegThreads) seg_count_kernel(const TorParams p, SegPlan sp) {
     extern __shared__ int hist[];  // [n_slabs]
+    __shared__ signed char owner_tab[kSegThreads / 32][32];
     for (int k = threadIdx.x; k < sp.n_slabs; k += kSegThreads) hist[k] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kSegTile;
     for (int it = 0; it < kSegItems; it++) {
         const int64_t t = base + (int64_t)it * kSegThreads + threadIdx.x;
-        if (t >= p.n) break;
+        if (base + (int64_t)it * kSegThreads >= p.n) break;  // warp-uniform (whole block)
         int packed = -1;
         LorConst L;
-        bool ok = geometry_any<OP>(p, t, L);  // generated map LORs are made here
-        if (ok) {  // only LORs that enter the slab lists are ever read back
-            const LorRec r = make_rec(L, ok);
-            float4 *q = reinterpret_cast<float4 *>(sp.rec + t);
-            q[0] = r.a;
-            q[1] = r.b;
-            q[2] = r.c;
-            q[3] = r.d;
+        bool ok = false;
+        SlabIdLor c{};
+        if (t < p.n) {
+            ok = geometry_any<OP>(p, t, L);  // generated map LORs are made here
+            if (ok) {  // only LORs that enter the slab lists are ever read back
+                const LorRec r = make_rec(L, ok);
+                float4 *q = reinterpret_cast<float4 *>(sp.rec + t);
+                q[0] = r.a;
+                q[1] = r.b;
+                q[2] = r.c;
+                q[3] = r.d;
+            }
+            if (ok && OP == kBack) ok = (double)__ldg(p.values + t) > 1e-7;  // tor.cu.cc:203
+            if (ok) {
+                const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
+                const int k_lo = f0 + L.s_lo / sp.nsl, k_hi = f0 + L.s_hi / sp.nsl;
+                packed = k_lo | (k_hi << 16);
+                c = slab_id_lor(p, sp, t, k_lo, k_hi, L.s_lo, L.s_hi, L.y1, L.z1, L.d1, L.dz);
+            }
+            sp.range[t] = packed;
         }
-        if (ok && OP == kBack) ok = (double)__ldg(p.values + t) > 1e-7;  // tor.cu.cc:203
-        if (ok) {
-            const int f0 = p.frame ? __ldg(p.frame + t) * sp.slabs_pf : 0;
-            const int k_lo = f0 + L.s_lo / sp.nsl, k_hi = f0 + L.s_hi / sp.nsl;
-            packed = k_lo | (k_hi << 16);
-            lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, L.s_lo, L.s_hi, L.y1, L.z1, L.d1, L.dz,
-                                [&](int id) { atomicAdd(&hist[id], 1); });
+        if (OP == kMap && kBand) {
+            warp_slab_ids<kBand>(p, sp, owner_tab[threadIdx.x >> 5], ok, (int)t, c,
+                                 [&](int id, int) { atomicAdd(&hist[id], 1); });
+        } else if (ok) {
+            for (int k = c.k_lo; k <= c.k_hi; k++)
+                range_slab_ids<kBand>(p, sp, c, k, [&](int id) { atomicAdd(&hist[id], 1); });
         }
-        sp.range[t] = packed;
     }
     __syncthreads();
     for (int k = threadIdx.x; k < sp.n_slabs; k += kSegThreads)
@@ -997,6 +1082,12 @@ __global__ void seg_offsets_kernel(SegPlan sp, const int64_t *slab_tot) {
     }
 }
 
+// Filling: one LOR per lane, so that the lanes of a warp that meet a slab append their
+// LORs to its list side by side, in LOR order (warp_increment). The slab kernels hand a warp
+// 32 consecutive entries of a list and walk the largest box among them: runs of
+// neighbouring LORs (records are ordered by direction) keep those warps coherent. Spread
+// over the lanes like the counting, the entries interleave and the slab kernels ran 4-8 %
+// slower (measured).
 template <bool kBand>
 __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p, SegPlan sp) {
     extern __shared__ int64_t tile_base[];  // [n_slabs] where this tile's run of each slab starts
@@ -1026,10 +1117,12 @@ __global__ void __launch_bounds__(kSegThreads) seg_fill_kernel(const TorParams p
             d1 = b.x;
             dz = b.y;
         }
-        lor_slab_ids<kBand>(p, sp, t, k_lo, k_hi, s_lo, s_hi, y1, z1, d1, dz, [&](int id) {
-            const int pos = warp_increment(cursor, id);
-            sp.seg[tile_base[id] + pos] = (int)t;
-        });
+        const SlabIdLor c = slab_id_lor(p, sp, t, k_lo, k_hi, s_lo, s_hi, y1, z1, d1, dz);
+        for (int k = k_lo; k <= k_hi; k++)
+            range_slab_ids<kBand>(p, sp, c, k, [&](int id) {
+                const int pos = warp_increment(cursor, id);
+                sp.seg[tile_base[id] + pos] = (int)t;
+            });
     }
 }
 
