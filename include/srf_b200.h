@@ -159,6 +159,21 @@ int srf_tor_projection_backprojection_batched(
     const float *size, float kernel_width, float tof_bin, float tof_sigma2, const float *images,
     float *back_images, int64_t num_events, int64_t lor_stride, int accumulate, void *stream);
 
+/* srf_tor_projection_backprojection_batched on image stacks in any axis order: voxel
+ * (ix, iy, iz) of frame f (the kernel's axes, grid[0..2]) is element f * frame_stride +
+ * ix * image_strides[0] + iy * image_strides[1] + iz * image_strides[2] (HOST int64[3],
+ * each >= 1, a frame's last voxel below frame_stride) of both images and back_images,
+ * e.g. a permuted view of an [F, nx, ny, nz] stack, which then needs no copy into the
+ * kernel layout and back. No counterpart in the reference. */
+int srf_tor_projection_backprojection_batched_strided(
+    const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
+    const float *z2, const float *xc, const float *yc, const float *zc,
+    const float *sigma2_factor, int geo_sigma2_flag, const int *frame, int n_frames,
+    int64_t frame_stride, float *projection_value, const int *grid, const float *center,
+    const float *size, float kernel_width, float tof_bin, float tof_sigma2, const float *images,
+    float *back_images, const int64_t *image_strides, int64_t num_events, int64_t lor_stride,
+    int accumulate, void *stream);
+
 /* No counterpart in the reference: batched TOR for many reconstructions that share one
  * geometry (dynamic frames, many phantoms). LOR i belongs to frame frame[i] (DEVICE
  * int32[N], 0 <= frame[i] < n_frames; a LOR with a frame id outside that range

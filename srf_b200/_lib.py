@@ -47,6 +47,9 @@ SIGNATURES = {
     "srf_tor_projection_backprojection_batched": (_TOR_COLS + [_int, _p, _int, _i64, _p, _p, _p,
                                                                _p, _f, _f, _f, _p, _p, _i64,
                                                                _i64, _int, _p], _int),
+    "srf_tor_projection_backprojection_batched_strided": (
+        _TOR_COLS + [_int, _p, _int, _i64, _p, _p, _p, _p, _f, _f, _f, _p, _p, _p, _i64, _i64,
+                     _int, _p], _int),
     "srf_tor_backproject_adjoint_batched": (_TOR_COLS + [_int, _p, _int, _i64, _p, _p, _p, _p,
                                                          _f, _f, _f, _p, _i64, _i64, _int, _p],
                                             _int),

@@ -94,6 +94,9 @@ class BatchedOSEM:
             g, c, s = self.geom[a]
             if lors.shape[0] == 0:
                 continue
+            # a copy into the group's layout: measured faster here than projecting through
+            # the permuted view (ops.tor_projection_backprojection_batched_strided): 176.6
+            # against 181.6 ms per 64-frame iteration at 96 x 96 x 48
             img_a = self.x.permute(*_stacked_perm(m.perm(a))).contiguous()
             _, bk = ops.tor_projection_backprojection_batched(
                 lors, frame, img_a, self.F, g, c, s, m.kernel_width, m.geo_sigma2_flag,

@@ -70,6 +70,10 @@ struct TorParams {
     const int *frame;
     int64_t frame_stride;
     int n_frames;
+    // Element strides of the kernel axes x, y, z inside a frame of image_in and image_out
+    // (1, gx, gx gy for a contiguous image; any layout whose frame fits in frame_stride,
+    // e.g. a permuted view of an image stack, through the strided entry point).
+    int64_t sx, sy, sz;
     // Map LORs made on the fly (srf_tor_maplors_generated): gen = 0 LOR columns in memory;
     // 1 uniform random crystal pairs; 2 every crystal pair of the scanner's block pairs.
     // LOR t of the call is number gen_first + t of that sequence, taken through
@@ -263,7 +267,6 @@ __device__ __noinline__ void generic_lor(const TorParams &p, int64_t t, int lane
         if (OP == kCount && lane == 0) p.count_out[t] = p.count_out[p.n + t] = 0;
         return;
     }
-    const int64_t slice_mesh = (int64_t)p.gx * p.gy;
     const int64_t img0 = frame_offset(p, t);
     const int64_t o = t * p.stride;
     float x1, y1, z1, x2, y2, z2, f;
@@ -341,14 +344,14 @@ __device__ __noinline__ void generic_lor(const TorParams &p, int64_t t, int lane
             const int i_lo = max(0, -ix0), i_hi = min(p.patch, p.gx - ix0);
             const int j_lo = max(0, -iy0), j_hi = min(p.patch, p.gy - iy0);
             if (OP == kCount) n_slots += max(0, i_hi - i_lo) * max(0, j_hi - j_lo);
-            const int64_t base = (int64_t)s * slice_mesh;
+            const int64_t base = (int64_t)s * p.sz;
             for (int j = j_lo; j < j_hi; ++j) {
                 const int iy = iy0 + j;
                 const float my = __fmaf_rn(p.inter_y, (float)iy + 0.5f, p.b_bound);
                 const float dy = __fsub_rn(cy, my);
                 const float dyuy = __fmul_rn(dy, uy);
                 const float dy2 = __fmul_rn(dy, dy);
-                const int64_t row = base + (int64_t)iy * p.gx;
+                const int64_t row = base + (int64_t)iy * p.sy;
                 for (int i = i_lo; i < i_hi; ++i) {
                     const int ix = ix0 + i;
                     const float mx = __fmaf_rn(p.inter_x, (float)ix + 0.5f, p.l_bound);
@@ -360,12 +363,12 @@ __device__ __noinline__ void generic_lor(const TorParams &p, int64_t t, int lane
                         if (OP == kCount) {
                             n_useful++;
                         } else if (OP == kProj) {
-                            acc = fmaf(w, __ldg(p.image_in + img0 + row + ix), acc);
+                            acc = fmaf(w, __ldg(p.image_in + img0 + row + ix * p.sx), acc);
                         } else {
-                            atomicAdd(p.image_out + img0 + row + ix, w * scale);
+                            atomicAdd(p.image_out + img0 + row + ix * p.sx, w * scale);
                         }
                     } else if (OP == kMap && all_slots) {
-                        atomicAdd(p.image_out + img0 + row + ix, 0.0f * scale);
+                        atomicAdd(p.image_out + img0 + row + ix * p.sx, 0.0f * scale);
                     }
                 }
             }
@@ -774,7 +777,6 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t slice_mesh = (int64_t)p.gx * p.gy;
     for (int64_t t = warp; t < p.n; t += nwarps) {
         LorConst L;
         const bool any = prepare_any<OP>(p, t, L);
@@ -783,10 +785,10 @@ __global__ void __launch_bounds__(256) tor_kernel_p(const TorParams p) {
         if (any) {
             const int64_t img0 = frame_offset(p, t);
             for (int s = L.s_lo + lane; s <= L.s_hi; s += 32) {
-                const int64_t base = img0 + (int64_t)s * slice_mesh;
+                const int64_t base = img0 + (int64_t)s * p.sz;
                 n_slots += slice_visit<OP, P, false, false>(p, L, s, 0, p.gy,
                                                      [&](int ix, int iy, float w, bool use) {
-                    const int64_t idx = base + (int64_t)iy * p.gx + ix;
+                    const int64_t idx = base + (int64_t)iy * p.sy + (int64_t)ix * p.sx;
                     if (OP == kCount) {
                         n_useful += use ? 1 : 0;
                     } else if (OP == kProj) {
@@ -1159,7 +1161,6 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
     __shared__ signed char owner_tab[kSlabThreads / 32][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int kWarps = kSlabThreads / 32;
-    const int slice_mesh = p.gx * p.gy;
     constexpr int pad = P - 1;
     const int rs = slab_row_stride(p.gx, pad), ss = slab_slice_stride(p.gx, sp.band_rows, pad);
     const int origin = slab_origin(p.gx, pad);
@@ -1196,12 +1197,23 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
         const int64_t img0 = (int64_t)fr * p.frame_stride;
         const int n_rows = (S1 - S0) * nbr;
         if (OP == kProj) {
-            const float *src = p.image_in + img0 + (int64_t)S0 * slice_mesh + (int64_t)R0 * p.gx;
-            for (int r = warp; r < n_rows; r += kWarps) {
-                const int sl = r / nbr, iy = r - sl * nbr;
-                const float *g = src + (int64_t)sl * slice_mesh + (int64_t)iy * p.gx;
-                float *d = slab + origin + sl * ss + iy * rs;
-                for (int ix = lane; ix < p.gx; ix += 32) d[ix] = __ldg(g + ix);
+            const float *src = p.image_in + img0 + (int64_t)S0 * p.sz + (int64_t)R0 * p.sy;
+            if (p.sx == 1 || p.sy != 1) {  // lanes along x (contiguous rows, or neither axis)
+                for (int r = warp; r < n_rows; r += kWarps) {
+                    const int sl = r / nbr, iy = r - sl * nbr;
+                    const float *g = src + (int64_t)sl * p.sz + (int64_t)iy * p.sy;
+                    float *d = slab + origin + sl * ss + iy * rs;
+                    for (int ix = lane; ix < p.gx; ix += 32) d[ix] = __ldg(g + (int64_t)ix * p.sx);
+                }
+            } else {  // y contiguous (a permuted view): a warp per column, lanes along y
+                for (int sl = 0; sl < S1 - S0; sl++) {
+                    const float *gs = src + (int64_t)sl * p.sz;
+                    float *ds = slab + origin + sl * ss;
+                    for (int ix = warp; ix < p.gx; ix += kWarps) {
+                        const float *g = gs + (int64_t)ix * p.sx;
+                        for (int iy = lane; iy < nbr; iy += 32) ds[iy * rs + ix] = __ldg(g + iy);
+                    }
+                }
             }
         } else {
             const int n = slab_floats(S1 - S0, p.gx, sp.band_rows, pad);
@@ -1310,14 +1322,28 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
         }
         __syncthreads();
         if (OP != kProj) {
-            float *out = p.image_out + img0 + (int64_t)S0 * slice_mesh + (int64_t)R0 * p.gx;
-            for (int r = warp; r < n_rows; r += kWarps) {
-                const int sl = r / nbr, iy = r - sl * nbr;
-                const float *src = slab + origin + sl * ss + iy * rs;
-                float *g = out + (int64_t)sl * slice_mesh + (int64_t)iy * p.gx;
-                for (int ix = lane; ix < p.gx; ix += 32) {
-                    const float v = src[ix];
-                    if (v != 0.0f) atomicAdd(g + ix, v);
+            float *out = p.image_out + img0 + (int64_t)S0 * p.sz + (int64_t)R0 * p.sy;
+            if (p.sx == 1 || p.sy != 1) {
+                for (int r = warp; r < n_rows; r += kWarps) {
+                    const int sl = r / nbr, iy = r - sl * nbr;
+                    const float *src = slab + origin + sl * ss + iy * rs;
+                    float *g = out + (int64_t)sl * p.sz + (int64_t)iy * p.sy;
+                    for (int ix = lane; ix < p.gx; ix += 32) {
+                        const float v = src[ix];
+                        if (v != 0.0f) atomicAdd(g + (int64_t)ix * p.sx, v);
+                    }
+                }
+            } else {
+                for (int sl = 0; sl < S1 - S0; sl++) {
+                    float *gs = out + (int64_t)sl * p.sz;
+                    const float *ds = slab + origin + sl * ss;
+                    for (int ix = warp; ix < p.gx; ix += kWarps) {
+                        float *g = gs + (int64_t)ix * p.sx;
+                        for (int iy = lane; iy < nbr; iy += 32) {
+                            const float v = ds[iy * rs + ix];
+                            if (v != 0.0f) atomicAdd(g + iy, v);
+                        }
+                    }
                 }
             }
             __syncthreads();
@@ -1371,6 +1397,9 @@ int tor_setup(TorParams &p, const int *grid, const float *center, const float *s
                            : 1.0f;
     p.inv_x = 1.0f / p.inter_x;
     p.inv_y = 1.0f / p.inter_y;
+    p.sx = 1;
+    p.sy = gx;
+    p.sz = (int64_t)gx * gy;
     // |dx|, |dy| <= patch * inter inside a window; the float d^2 of such a voxel is within
     // ~1e-6 (patch * inter)^2 of the exact value, the margin is 2^-16 (patch * inter)^2.
     const float span = (float)p.patch * std::max(p.inter_x, p.inter_y);
@@ -1972,6 +2001,55 @@ extern "C" int srf_tor_projection_backprojection_batched(
     pp.x1 = x1; pp.y1 = y1; pp.z1 = z1; pp.x2 = x2; pp.y2 = y2; pp.z2 = z2;
     pp.xc = xc; pp.yc = yc; pp.zc = zc; pp.f = sigma2_factor;
     pp.geo = geo_sigma2_flag != 0;
+    TorParams pb = pp;
+    pp.image_in = images;
+    pp.proj_out = projection_value;
+    pb.values = projection_value;
+    pb.image_out = back_images;
+    return tor_launch_pair(pp, pb, (cudaStream_t)stream);
+}
+
+// srf_tor_projection_backprojection_batched on image stacks in any axis order: voxel
+// (ix, iy, iz) of frame f (kernel axes) is at f * frame_stride + ix image_strides[0] +
+// iy image_strides[1] + iz image_strides[2] of both images and back_images, e.g. a
+// permuted view of an [F, nx, ny, nz] stack, which then needs no copy into the kernel
+// layout and back.
+extern "C" int srf_tor_projection_backprojection_batched_strided(
+    const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
+    const float *z2, const float *xc, const float *yc, const float *zc,
+    const float *sigma2_factor, int geo_sigma2_flag, const int *frame, int n_frames,
+    int64_t frame_stride, float *projection_value, const int *grid, const float *center,
+    const float *size, float kernel_width, float tof_bin, float tof_sigma2, const float *images,
+    float *back_images, const int64_t *image_strides, int64_t num_events, int64_t lor_stride,
+    int accumulate, void *stream) {
+    TorParams pp{};
+    int st = tor_setup(pp, grid, center, size, kernel_width, tof_bin, tof_sigma2, num_events,
+                       lor_stride);
+    if (st != SRF_OK) return st;
+    if ((st = set_frames(pp, frame, n_frames, frame_stride)) != SRF_OK) return st;
+    if (!image_strides) return SRF_ERR_INVALID_ARGUMENT;
+    const int64_t sx = image_strides[0], sy = image_strides[1], sz = image_strides[2];
+    if (sx < 1 || sy < 1 || sz < 1) return SRF_ERR_INVALID_ARGUMENT;
+    // a frame's voxels stay inside its frame_stride floats (and the offsets inside int64)
+    const int64_t lim = (int64_t)1 << 40;
+    if (sx > lim || sy > lim || sz > lim) return SRF_ERR_UNSUPPORTED;
+    if ((int64_t)(pp.gx - 1) * sx + (int64_t)(pp.gy - 1) * sy + (int64_t)(pp.gz - 1) * sz >=
+        frame_stride)
+        return SRF_ERR_INVALID_ARGUMENT;
+    if (!back_images || back_images == images) return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > 0 &&
+        !cols_ok({x1, y1, z1, x2, y2, z2, sigma2_factor, projection_value, images}))
+        return SRF_ERR_INVALID_ARGUMENT;
+    if (num_events > 0 && pp.tof_on && !cols_ok({xc, yc, zc})) return SRF_ERR_INVALID_ARGUMENT;
+    if (!accumulate &&
+        (st = zero_frames(back_images, n_frames, frame_stride, (cudaStream_t)stream)) != SRF_OK)
+        return st;
+    pp.x1 = x1; pp.y1 = y1; pp.z1 = z1; pp.x2 = x2; pp.y2 = y2; pp.z2 = z2;
+    pp.xc = xc; pp.yc = yc; pp.zc = zc; pp.f = sigma2_factor;
+    pp.geo = geo_sigma2_flag != 0;
+    pp.sx = sx;
+    pp.sy = sy;
+    pp.sz = sz;
     TorParams pb = pp;
     pp.image_in = images;
     pp.proj_out = projection_value;

@@ -411,6 +411,46 @@ def tor_projection_backprojection_batched(lors, frame, images, n_frames, grid, c
     return out_values, out
 
 
+def tor_projection_backprojection_batched_strided(lors, frame, images, back, grid, center,
+                                                  size, kernel_width, geo_sigma2_flag=False,
+                                                  tof_bin=1.0e4, tof_sigma2=1.0e4,
+                                                  layout="auto", out_values=None,
+                                                  accumulate=True):
+    """``tor_projection_backprojection_batched`` on image stacks in any axis order:
+    ``images`` and ``back`` are [F, gz, gy, gx] views (the kernel's axes, e.g. a permuted
+    view of an [F, nx, ny, nz] stack) with the same strides; ``back`` += the
+    back-projection (zeroed first unless ``accumulate``). Returns the projected values."""
+    dev = _check_cuda(lors, images, back, out_values)
+    t, cols, n, stride = _columns(lors, TOR_COLS, layout)
+    g, ga, ca, sa = _geom(grid, center, size)
+    if images.dim() != 4 or tuple(images.shape[1:]) != (g[2], g[1], g[0]):
+        raise ValueError("images must be an [F, gz, gy, gx] view")
+    if back.shape != images.shape or back.stride() != images.stride():
+        raise ValueError("back must be a view of the same shape and strides as images")
+    if images.dtype != torch.float32 or back.dtype != torch.float32:
+        raise TypeError("images must be float32")
+    import ctypes as C
+    n_frames = int(images.shape[0])
+    fs = int(images.stride(0))
+    fr, _ = _frame_args(frame, n_frames, images.numel(), g)
+    if fr.numel() != n:
+        raise ValueError("frame needs one entry per LOR")
+    if back.data_ptr() == images.data_ptr():
+        raise ValueError("the back-projection must not overwrite the projected images")
+    if out_values is None:
+        out_values = torch.empty(n, dtype=torch.float32, device=dev)
+    elif out_values.numel() != n or not out_values.is_contiguous():
+        raise ValueError("out_values must be a contiguous tensor with one entry per LOR")
+    st = (C.c_int64 * 3)(int(images.stride(3)), int(images.stride(2)), int(images.stride(1)))
+    with torch.cuda.device(dev):
+        _call(dev, "srf_tor_projection_backprojection_batched_strided", *cols[:10],
+              int(bool(geo_sigma2_flag)), fr.data_ptr(), n_frames, fs, out_values.data_ptr(),
+              ga, ca, sa, float(kernel_width), float(tof_bin), float(tof_sigma2),
+              images.data_ptr(), back.data_ptr(), st, n, stride, int(bool(accumulate)),
+              _stream(dev))
+    return out_values
+
+
 def _tor_scatter_batched(fn, lors, frame, values, n_frames, grid, center, size, kernel_width,
                          geo_sigma2_flag, tof_bin, tof_sigma2, layout, out, accumulate):
     dev = _check_cuda(lors, values, out)

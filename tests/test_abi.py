@@ -82,3 +82,27 @@ def test_new_entry_points_validate_before_any_launch():
     assert f(1, None, 2, 2, 1, 0, 5, 2, 0, 0, g, c, s, 1.0, None, 0, None) == 1
     assert lib.srf_siddon_set_tuning(2) == 1
     assert lib.srf_siddon_set_tuning(0) == 0
+
+
+def test_strided_batched_call_validates_strides():
+    """The strided batched call rejects missing, non-positive and frame-overrunning image
+    strides on the host (status 1), before any launch."""
+    lib = _lib.load()
+    g = (ctypes.c_int * 3)(4, 5, 6)
+    c = (ctypes.c_float * 3)(0, 0, 0)
+    s = (ctypes.c_float * 3)(1, 1, 1)
+    f = lib.srf_tor_projection_backprojection_batched_strided
+
+    def call(strides, frame_stride=120):
+        st = None if strides is None else (ctypes.c_int64 * 3)(*strides)
+        # 0 events: no LOR columns needed; images / back_images distinct dummy addresses
+        return f(*([None] * 10), 0, None, 2, frame_stride, None, g, c, s, 1.0, 1.0, 1.0,
+                 ctypes.c_void_p(4096), ctypes.c_void_p(8192), st, 0, 1, 1, None)
+
+    assert call(None) == 1
+    assert call((0, 4, 20)) == 1
+    assert call((1, -4, 20)) == 1
+    # the frame's last voxel (3 + 4 * 4 + 5 * 30 = 169) must lie below frame_stride
+    assert call((1, 4, 30), frame_stride=160) == 1
+    # a frame_stride below the grid's voxel count is rejected as for the batched calls
+    assert call((1, 4, 20), frame_stride=100) == 1

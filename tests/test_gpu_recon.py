@@ -182,6 +182,16 @@ def test_batched_ops_equal_per_frame(tune):
                 lors, frame, stack, len(frames), g, c, s, K.KW_CONFIG, False, b, s2, layout="nc")
             assert K.rel_l2(pv2.cpu().numpy(), pv.cpu().numpy()) < 1e-6
             assert K.rel_l2(bp2.cpu().numpy(), bp.cpu().numpy()) < 1e-6
+            # the same through permuted views of the [F, nx, ny, nz] stack (no copies), the
+            # back-projection added into a stack that already holds values
+            stored = cu(np.stack(imgs))
+            sp = [0] + [d + 1 for d in perm]
+            back = torch.full_like(stored, 0.5)
+            pv3 = ops.tor_projection_backprojection_batched_strided(
+                lors, frame, stored.permute(*sp), back.permute(*sp), g, c, s, K.KW_CONFIG,
+                False, b, s2, layout="nc")
+            assert K.rel_l2(pv3.cpu().numpy(), pv.cpu().numpy()) < 1e-6
+            assert K.rel_l2((back.permute(*sp) - 0.5).cpu().numpy(), bp.cpu().numpy()) < 1e-6
     finally:
         tuning.set_tuning()
 
