@@ -228,7 +228,7 @@ int srf_tor_set_tuning(int path, int slab_slices, int grid_mult);
 int srf_siddon_set_tuning(int path);
 
 /* No counterpart in the reference: upper bound, in bytes, of the per-slab LOR lists the
- * slab kernels build per call (0 = the default, 1 GiB). The lists are sized for the worst
+ * slab kernels build per call (0 = the default, 4 GiB). The lists are sized for the worst
  * case, 4 bytes x LORs x slabs per frame; a call with more LORs than fit is processed in
  * chunks of LORs (at least 4096 each), each chunk a complete pass. Process-wide. */
 int srf_tor_set_scratch_limit(int64_t bytes);

@@ -841,8 +841,14 @@ constexpr int kSegTile = kSegThreads * kSegItems;
 constexpr int kMaxSlabs = 4096;
 constexpr int kSlabThreads = 1024;
 constexpr size_t kSlabSmemBytes = 220 * 1024;  // of the 227 KB a CTA can opt into
-// Budget of the per-slab LOR lists of one chunk of LORs (srf_tor_set_scratch_limit).
-std::atomic<long long> g_seg_scratch_bytes{1ll << 30};
+// Budget of the per-slab LOR lists of one chunk of LORs (srf_tor_set_scratch_limit). The
+// lists are sized for the worst case (every slab of a frame), so the budget sets how many
+// chunks a call over row-band slabs takes, each a full pass (slab loads and flushes again):
+// 10M events at 256 x 256 x 128 24.1 ms per combined call with 1 GiB, 20.9 with 2, 19.0
+// with 4 (5 -> 2 chunks per group); 50M generated map LORs 242 / 221 / 208 ms. 4 GiB is
+// 2 % of a B200's memory, held by the library's pool once a call has needed it.
+constexpr long long kSegScratchDefault = 4ll << 30;
+std::atomic<long long> g_seg_scratch_bytes{kSegScratchDefault};
 
 struct SegPlan {
     int nsl, n_slabs, ntiles;  // n_slabs counts slab ids over all frames
@@ -2078,7 +2084,7 @@ extern "C" int srf_tor_backproject_adjoint_batched(
 // automatic).
 extern "C" int srf_tor_set_scratch_limit(int64_t bytes) {
     if (bytes < 0) return SRF_ERR_INVALID_ARGUMENT;
-    g_seg_scratch_bytes.store(bytes == 0 ? (1ll << 30) : (long long)bytes);
+    g_seg_scratch_bytes.store(bytes == 0 ? kSegScratchDefault : (long long)bytes);
     return SRF_OK;
 }
 

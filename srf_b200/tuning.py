@@ -38,7 +38,7 @@ def set_siddon_tuning(path=0):
 
 def set_scratch_limit(nbytes=0):
     """Bound the per-call scratch of the slab kernels (``srf_tor_set_scratch_limit``);
-    larger calls run in chunks of LORs. 0 restores the default (1 GiB)."""
+    larger calls run in chunks of LORs. 0 restores the default (4 GiB)."""
     _lib.call("srf_tor_set_scratch_limit", int(nbytes))
 
 
