@@ -1204,22 +1204,11 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
         const int n_rows = (S1 - S0) * nbr;
         if (OP == kProj) {
             const float *src = p.image_in + img0 + (int64_t)S0 * p.sz + (int64_t)R0 * p.sy;
-            if (p.sx == 1 || p.sy != 1) {  // lanes along x (contiguous rows, or neither axis)
-                for (int r = warp; r < n_rows; r += kWarps) {
-                    const int sl = r / nbr, iy = r - sl * nbr;
-                    const float *g = src + (int64_t)sl * p.sz + (int64_t)iy * p.sy;
-                    float *d = slab + origin + sl * ss + iy * rs;
-                    for (int ix = lane; ix < p.gx; ix += 32) d[ix] = __ldg(g + (int64_t)ix * p.sx);
-                }
-            } else {  // y contiguous (a permuted view): a warp per column, lanes along y
-                for (int sl = 0; sl < S1 - S0; sl++) {
-                    const float *gs = src + (int64_t)sl * p.sz;
-                    float *ds = slab + origin + sl * ss;
-                    for (int ix = warp; ix < p.gx; ix += kWarps) {
-                        const float *g = gs + (int64_t)ix * p.sx;
-                        for (int iy = lane; iy < nbr; iy += 32) ds[iy * rs + ix] = __ldg(g + iy);
-                    }
-                }
+            for (int r = warp; r < n_rows; r += kWarps) {
+                const int sl = r / nbr, iy = r - sl * nbr;
+                const float *g = src + (int64_t)sl * p.sz + (int64_t)iy * p.sy;
+                float *d = slab + origin + sl * ss + iy * rs;
+                for (int ix = lane; ix < p.gx; ix += 32) d[ix] = __ldg(g + (int64_t)ix * p.sx);
             }
         } else {
             const int n = slab_floats(S1 - S0, p.gx, sp.band_rows, pad);
@@ -1329,27 +1318,13 @@ __global__ void __launch_bounds__(kSlabThreads, 1) tor_slab_kernel(const TorPara
         __syncthreads();
         if (OP != kProj) {
             float *out = p.image_out + img0 + (int64_t)S0 * p.sz + (int64_t)R0 * p.sy;
-            if (p.sx == 1 || p.sy != 1) {
-                for (int r = warp; r < n_rows; r += kWarps) {
-                    const int sl = r / nbr, iy = r - sl * nbr;
-                    const float *src = slab + origin + sl * ss + iy * rs;
-                    float *g = out + (int64_t)sl * p.sz + (int64_t)iy * p.sy;
-                    for (int ix = lane; ix < p.gx; ix += 32) {
-                        const float v = src[ix];
-                        if (v != 0.0f) atomicAdd(g + (int64_t)ix * p.sx, v);
-                    }
-                }
-            } else {
-                for (int sl = 0; sl < S1 - S0; sl++) {
-                    float *gs = out + (int64_t)sl * p.sz;
-                    const float *ds = slab + origin + sl * ss;
-                    for (int ix = warp; ix < p.gx; ix += kWarps) {
-                        float *g = gs + (int64_t)ix * p.sx;
-                        for (int iy = lane; iy < nbr; iy += 32) {
-                            const float v = ds[iy * rs + ix];
-                            if (v != 0.0f) atomicAdd(g + iy, v);
-                        }
-                    }
+            for (int r = warp; r < n_rows; r += kWarps) {
+                const int sl = r / nbr, iy = r - sl * nbr;
+                const float *src = slab + origin + sl * ss + iy * rs;
+                float *g = out + (int64_t)sl * p.sz + (int64_t)iy * p.sy;
+                for (int ix = lane; ix < p.gx; ix += 32) {
+                    const float v = src[ix];
+                    if (v != 0.0f) atomicAdd(g + (int64_t)ix * p.sx, v);
                 }
             }
             __syncthreads();
