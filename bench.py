@@ -1092,8 +1092,9 @@ def _pick(d, *keys):
 
 
 def run_other_configs():
-    """The other BASELINE configurations, each run in this process after the default
-    step's measurement, summarised (their full lines come from ``--workload NAME``)."""
+    """The other benchmark workloads (Siddon 64^3, batched frames, the differentiable
+    projector, the large axial FOV), each run in this process after the default step's
+    measurement, summarised (their full lines come from ``--workload NAME``)."""
     global _COLLECT
     plan = [
         ("config1_siddon64", ["--workload", "siddon64"],
