@@ -87,14 +87,28 @@ def _oracle_map(model, lors, grid, center, size):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["random128", "random256band", "blockpairs"])
+@pytest.mark.parametrize("case", ["random128", "random256band", "random256bands_xy",
+                                  "blockpairs"])
 def test_fused_map_equals_materialised_and_oracle(case):
+    """random256band: the z group's 256 x 256 slices need row bands; random256bands_xy: 16-slice
+    slabs force row bands on the x and y groups too, whose map binning then spreads its
+    (LOR, slice range) items over the lanes."""
+    from srf_b200 import tuning
+    if case == "random256bands_xy":
+        tuning.set_tuning(1, 16, 0)
+    try:
+        _fused_map_case(case)
+    finally:
+        tuning.set_tuning()
+
+
+def _fused_map_case(case):
     from srf_b200 import SplitLoRsModel, recon
     from tests import _cases as K
     if case == "blockpairs":
         src = GeneratedPairs.block_pairs(small_pet(), chunk=3000)
         grid, voxel = (24, 24, 4), 8.0
-    elif case == "random256band":
+    elif case.startswith("random256"):
         src = GeneratedPairs.random(RingScanner(390.0, 600, 320, 3.125), 20_000, 3, chunk=7000)
         grid, voxel = (256, 256, 16), 2.5
     else:
