@@ -50,3 +50,23 @@ def test_opposite_blocks_lor():
                         block_size=[6.0, 2.0, 1.0])
     np.testing.assert_allclose(sc.make_ring_pairs_lors(0, 0), [[1.0, 0, 0, -1.0, 0, 0]],
                                atol=1e-12)
+
+
+def test_tof_info_known_answers():
+    """tof_info restates _get_tof_info (src/python/srf/api/app/srfapp_new.py:244-251): the
+    3-sigma limit res * 0.15 / 2.35482005 * 3 mm, sigma^2 = limit^2 / 9, bin * 0.15 mm. The
+    workloads' figures: 530 ps FWHM -> sigma 33.76 mm (sigma^2 1139.774), 400 ps -> 25.48 mm
+    (649.213), 40 ps bins -> 6 mm."""
+    import math
+    from srf_b200.scanner import tof_info
+    b, s2 = tof_info(530.0, 40.0)
+    assert b == 6.0
+    assert abs(s2 - 1139.7741617120942) < 1e-9
+    assert abs(math.sqrt(s2) - 33.76) < 5e-3
+    b, s2 = tof_info(400.0, 40.0)
+    assert b == 6.0
+    assert abs(s2 - 649.2127656601461) < 1e-9
+    assert abs(math.sqrt(s2) - 25.48) < 5e-3
+    # the same operations, in the reference's order
+    limit = 530.0 * 0.15 / 2.35482005 * 3
+    assert tof_info(530.0, 40.0)[1] == (limit ** 2) / 9
