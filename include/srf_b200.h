@@ -164,7 +164,9 @@ int srf_tor_projection_backprojection_batched(
  * ix * image_strides[0] + iy * image_strides[1] + iz * image_strides[2] (HOST int64[3],
  * each >= 1, a frame's last voxel below frame_stride) of both images and back_images,
  * e.g. a permuted view of an [F, nx, ny, nz] stack, which then needs no copy into the
- * kernel layout and back. No counterpart in the reference. */
+ * kernel layout and back. accumulate = 0 zeroes all n_frames * frame_stride floats from
+ * back_images first (the whole stack, not only the voxels the strides reach). No
+ * counterpart in the reference. */
 int srf_tor_projection_backprojection_batched_strided(
     const float *x1, const float *y1, const float *z1, const float *x2, const float *y2,
     const float *z2, const float *xc, const float *yc, const float *zc,
