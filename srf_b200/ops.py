@@ -419,7 +419,8 @@ def tor_projection_backprojection_batched_strided(lors, frame, images, back, gri
     """``tor_projection_backprojection_batched`` on image stacks in any axis order:
     ``images`` and ``back`` are [F, gz, gy, gx] views (the kernel's axes, e.g. a permuted
     view of an [F, nx, ny, nz] stack) with the same strides; ``back`` += the
-    back-projection (zeroed first unless ``accumulate``). Returns the projected values."""
+    back-projection (unless ``accumulate``, all F x stride(0) floats from its base are
+    zeroed first). Returns the projected values."""
     dev = _check_cuda(lors, images, back, out_values)
     t, cols, n, stride = _columns(lors, TOR_COLS, layout)
     g, ga, ca, sa = _geom(grid, center, size)
